@@ -1,0 +1,124 @@
+"""Seeded synthetic cell batches for the benchmark workloads.
+
+The reference's own timing dataset (``ref_data/res_gri3.0.csv``, a 55,076-cell
+GRI-Mech 3.0 triple flame) is not distributed with it, so seeded synthetic
+states with the benchmark's shapes and distributions stand in for it.  The
+mixture rule follows the reference's generator ``ref_data/generate.py:25``:
+fuel/air at equivalence ratio phi with air = O2 + 3.76 N2, converted from mole
+to mass fractions with the mechanism's molecular weights.
+
+Workloads (all rtol 1e-6, atol 1e-10):
+  h2_1024      h2o2,   1,024 cells, P = 101325 Pa, T0 ~ U[1000,1500] K, phi ~ U[0.5,2.0], dt 1e-3 s
+  gri_32k      gri30, 32,768 cells, P ~ U[1,10] atm, T0 ~ U[1000,1800] K, phi ~ U[0.5,1.5], dt 1e-4 s
+  gri_bimodal  gri30, 262,144 cells, P = 101325 Pa, T0 70% U[300,900] / 30% U[1100,2200] K,
+               phi log-uniform [0.3,3.0], dt 1e-4 s
+  gri_1m       gri30, 1,048,576 cells, P ~ U[1,40] atm, T0 ~ U[900,2400] K, phi ~ U[0.4,2.5], dt 1e-4 s
+"""
+from __future__ import annotations
+
+import json
+import os
+from dataclasses import dataclass
+from typing import Dict, Optional
+
+import numpy as np
+
+MECH_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "mech")
+ATM = 101325.0
+
+
+def mech_info(mech: str) -> Dict:
+    base = mech[:-5] if mech.endswith(".yaml") else mech
+    with open(os.path.join(MECH_DIR, f"{base}_mech.json")) as f:
+        return json.load(f)
+
+
+@dataclass
+class Batch:
+    mech: str
+    T: np.ndarray        # [n]
+    Y: np.ndarray        # [nsp, n]  species-major (cell index innermost), all species
+    P: np.ndarray        # [n]
+    dt: float
+    seed: int
+    name: str
+
+    @property
+    def ncells(self) -> int:
+        return self.T.size
+
+    @property
+    def nsp(self) -> int:
+        return self.Y.shape[0]
+
+    def state_rows(self) -> np.ndarray:
+        """Cell-major [n, nsp] integrator state [T, Y_0..Y_{nsp-2}] (reference layout)."""
+        return np.concatenate([self.T[:, None], self.Y[:-1].T], axis=1).copy()
+
+    def subset(self, idx) -> "Batch":
+        return Batch(self.mech, self.T[idx].copy(), self.Y[:, idx].copy(), self.P[idx].copy(),
+                     self.dt, self.seed, self.name + "[sub]")
+
+
+def premixed_Y(mech: str, fuel: str, phi: np.ndarray) -> np.ndarray:
+    """Mass fractions [nsp, n] of fuel/air at equivalence ratios phi."""
+    info = mech_info(mech)
+    names = info["species"]
+    mw = np.asarray(info["mw"])
+    idx = {s: i for i, s in enumerate(names)}
+    n = phi.size
+    X = np.zeros((len(names), n))
+    if fuel == "H2":
+        X[idx["H2"]] = 2.0 * phi
+        X[idx["O2"]] = 1.0
+        X[idx["N2"]] = 3.76
+    elif fuel == "CH4":
+        X[idx["CH4"]] = phi
+        X[idx["O2"]] = 2.0
+        X[idx["N2"]] = 7.52
+    else:
+        raise ValueError(fuel)
+    Ym = X * mw[:, None]
+    return Ym / Ym.sum(axis=0, keepdims=True)
+
+
+def make(name: str, ncells: Optional[int] = None, seed: Optional[int] = None) -> Batch:
+    """Build a named workload (optionally with fewer cells, same distributions)."""
+    cfg = WORKLOADS[name]
+    n = int(ncells if ncells is not None else cfg["ncells"])
+    sd = int(seed if seed is not None else cfg["seed"])
+    rng = np.random.default_rng(sd)
+    kind = cfg["kind"]
+    if kind == "h2":
+        T = rng.uniform(1000.0, 1500.0, n)
+        phi = rng.uniform(0.5, 2.0, n)
+        P = np.full(n, ATM)
+        Y = premixed_Y("h2o2", "H2", phi)
+        mech = "h2o2"
+    elif kind == "gri":
+        T = rng.uniform(cfg["T"][0], cfg["T"][1], n)
+        phi = rng.uniform(cfg["phi"][0], cfg["phi"][1], n)
+        P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
+        Y = premixed_Y("gri30", "CH4", phi)
+        mech = "gri30"
+    elif kind == "gri_bimodal":
+        cold = rng.uniform(0.0, 1.0, n) < 0.7
+        T = np.where(cold, rng.uniform(300.0, 900.0, n), rng.uniform(1100.0, 2200.0, n))
+        phi = np.exp(rng.uniform(np.log(0.3), np.log(3.0), n))
+        P = np.full(n, ATM)
+        Y = premixed_Y("gri30", "CH4", phi)
+        mech = "gri30"
+    else:
+        raise ValueError(kind)
+    return Batch(mech, T, Y, P, float(cfg["dt"]), sd, name)
+
+
+WORKLOADS = {
+    "h2_1024": dict(kind="h2", ncells=1024, dt=1e-3, seed=1),
+    "gri_32k": dict(kind="gri", ncells=32768, dt=1e-4, seed=2, T=(1000.0, 1800.0),
+                    phi=(0.5, 1.5), P_atm=(1.0, 10.0)),
+    "gri_bimodal": dict(kind="gri_bimodal", ncells=262144, dt=1e-4, seed=3),
+    "gri_1m": dict(kind="gri", ncells=1048576, dt=1e-4, seed=5, T=(900.0, 2400.0),
+                   phi=(0.4, 2.5), P_atm=(1.0, 40.0)),
+}
+RTOL, ATOL = 1e-6, 1e-10
