@@ -1,0 +1,769 @@
+// b200ode: kernels and C ABI (include/b200ode.h).
+//
+// Execution model (sm_100a):
+//   * one warp integrates one cell with the CVODE-semantics BDF of bdf_warp.cuh;
+//   * persistent form: a grid sized to the SM count x resident CTAs, every warp
+//     pulls cell indices from a device work queue (one 64-bit atomic per cell)
+//     and refills itself until the queue is empty, so cells of very different
+//     stiffness (a few vs hundreds of steps) never leave lanes idle;
+//   * one-launch-per-step form (the plain FP64 comparison form): every launch
+//     advances each unfinished cell by one BDF step, state kept in HBM between
+//     launches (k_bdf with per-cell records);
+//   * state in HBM is structure-of-arrays with the cell index innermost.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/b200ode.h"
+#include "bdf_warp.cuh"
+#include "mech/gri30_mech.h"
+#include "mech/h2o2_mech.h"
+
+using namespace b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+std::mutex g_tables_mu;
+std::map<std::pair<int, int>, unsigned char*> g_tables;   // (device, mechanism) -> tables
+
+b200ode_status fail(b200ode_status st, const std::string& msg) {
+    g_last_error = msg;
+    return st;
+}
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            return fail(B200ODE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define GEN_TABLES(tag, PFX)                                                                         \
+    GenTables{#tag, PFX##_NSP, PFX##_NRXN, PFX##_MAXP, PFX##_NTB, tag##_species_names, tag##_mw,      \
+              tag##_tmid, tag##_nasa_lo, tag##_nasa_hi, tag##_rxn_type, tag##_rxn_rev, tag##_rxn_A,   \
+              tag##_rxn_logA, tag##_rxn_b, tag##_rxn_EaR, tag##_rxn_A0, tag##_rxn_logA0, tag##_rxn_b0, \
+              tag##_rxn_EaR0, tag##_rxn_troe, tag##_rxn_troe_T2, tag##_rxn_reac_sp,                   \
+              tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp,  \
+              tag##_tb_alpha}
+
+enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1 };
+
+using GriT = MechT<MECH_GRI30_NSP, MECH_GRI30_NRXN, MECH_GRI30>;
+using H2T = MechT<MECH_H2O2_NSP, MECH_H2O2_NRXN, MECH_H2O2>;
+
+int mech_from_name(const char* name) {
+    if (!name) return -1;
+    std::string s(name);
+    if (s.size() > 5 && s.substr(s.size() - 5) == ".yaml") s = s.substr(0, s.size() - 5);
+    if (s == "gri30") return MECH_GRI30;
+    if (s == "h2o2") return MECH_H2O2;
+    return -1;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- kernels
+struct KParams {
+    long long ncells;
+    const double* P;
+    double P_scalar;
+    double* T;
+    double* Y;
+    int32_t* status;
+    int32_t* cnt[7];                  // per-cell counters (each may be null)
+    unsigned long long* queue;        // persistent form: work-queue head
+    unsigned long long* totals;       // [8] call totals
+    unsigned long long* prof;         // [5] per-phase cycle totals, or null
+    void* wglobal;                    // WarpGlobal per resident warp (persistent) or per cell (step form)
+    unsigned char* records;           // step form: per-cell state records; null = persistent form
+    unsigned long long* done_count;   // step form: cells finished
+    double t0, t1, rtol, atol;
+    int max_steps, max_order, refine, steps;
+};
+
+template <class MT>
+__device__ __forceinline__ void load_cell(const KParams& p, long long cell, int lane, double (&y0)[MT::NS]) {
+    constexpr int N = MT::N;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) y0[s] = p.Y[(long long)i * p.ncells + cell];
+        else if (i == N - 1) y0[s] = p.T[cell];
+        else y0[s] = 0.0;
+    }
+}
+
+template <class MT>
+__device__ __forceinline__ void store_cell(const KParams& p, long long cell, int lane, const double (&yo)[MT::NS]) {
+    constexpr int N = MT::N;
+    double part = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) part += yo[s];
+    }
+    const double yN = 1.0 - warp_sum(part);
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) p.Y[(long long)i * p.ncells + cell] = yo[s];
+        else if (i == N - 1) {
+            p.T[cell] = yo[s];
+            p.Y[(long long)(N - 1) * p.ncells + cell] = yN;
+        }
+    }
+}
+
+// The BDF kernel, both forms:
+//   persistent (records == null): a grid of resident warps; each warp pulls
+//     cell indices from the device work queue and integrates each cell to t1;
+//   one launch per step (records != null): warp w owns cell w and advances it by
+//     at most `steps` BDF steps, its full state kept in HBM between launches.
+// The step code is inlined once, so both forms execute the same instructions
+// and give the same bits.
+// MINB: minimum resident 128-thread blocks per SM the register allocation must
+// allow (1 -> up to 255 registers, 3 -> at most 168); chosen by the autotuner.
+template <class MT, class LinT, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KParams p) {
+    using B = WarpBdf<MT, LinT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    const bool step_form = p.records != nullptr;
+    auto* wglob = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal);
+    B bdf(sm, wglob + gw, lane);
+    bdf.rtol = p.rtol;
+    bdf.atol = p.atol;
+    bdf.max_steps = p.max_steps;
+    bdf.qmax = p.max_order;
+    bdf.refine = p.refine;
+    bdf.profiling = p.prof != nullptr;
+    if (lane < 8) sm->prof[lane] = 0;
+    __syncwarp();
+    const long long t_start = bdf.profiling ? clock64() : 0;
+    unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    long long cell = gw;
+#pragma unroll 1
+    for (int iter = 0;; ++iter) {
+        if (step_form) {
+            if (iter > 0 || cell >= p.ncells) break;
+        } else {
+            unsigned long long c = 0;
+            if (lane == 0) c = atomicAdd(p.queue, 1ULL);
+            c = __shfl_sync(kFull, c, 0);
+            if (c >= (unsigned long long)p.ncells) break;
+            cell = (long long)c;
+        }
+        unsigned char* rec = step_form ? p.records + cell * (long long)B::kRecordBytes : nullptr;
+        int phase = step_form ? reinterpret_cast<const typename B::Scalars*>(rec)->phase : 0;
+        if (phase == 2) continue;
+        int status = 0;
+        bool done = false;
+        bdf.lu_dirty = 0;
+        if (phase == 0) {
+            double y0[MT::NS];
+            load_cell<MT>(p, cell, lane, y0);
+            bdf.P = p.P ? p.P[cell] : p.P_scalar;
+            status = bdf.begin(y0, p.t0, p.t1);
+            done = (status != 0);
+        } else {
+            bdf.load(rec, status, phase);
+        }
+        if (!done) status = bdf.advance(p.t1, p.steps, done);
+        if (done) {
+            double yo[MT::NS];
+            bdf.finish(status, p.t1, yo);
+            store_cell<MT>(p, cell, lane, yo);
+            const CellCounters& c = bdf.cnt;
+            if (lane == 0) {
+                if (p.status) p.status[cell] = status;
+                if (p.cnt[0]) p.cnt[0][cell] = c.nst;
+                if (p.cnt[1]) p.cnt[1][cell] = c.nfe;
+                if (p.cnt[2]) p.cnt[2][cell] = c.nje;
+                if (p.cnt[3]) p.cnt[3][cell] = c.nsetups;
+                if (p.cnt[4]) p.cnt[4][cell] = c.nni;
+                if (p.cnt[5]) p.cnt[5][cell] = c.ncfn;
+                if (p.cnt[6]) p.cnt[6][cell] = c.netf;
+                if (step_form) atomicAdd(p.done_count, 1ULL);
+            }
+            tot[0] += c.nst; tot[1] += c.nfe; tot[2] += c.nje; tot[3] += c.nsetups;
+            tot[4] += c.nni; tot[5] += c.ncfn; tot[6] += c.netf; tot[7] += (status != 0);
+        }
+        if (step_form) bdf.save(rec, status, done ? 2 : 1, bdf.lu_dirty != 0);
+    }
+    if (lane == 0)
+        for (int i = 0; i < 8; ++i)
+            if (tot[i]) atomicAdd(p.totals + i, tot[i]);
+    if (bdf.profiling && lane == 0) {
+        sm->prof[PH_TOTAL] = clock64() - t_start;
+        for (int i = 0; i < 5; ++i) atomicAdd(p.prof + i, (unsigned long long)sm->prof[i]);
+    }
+}
+
+// Batched chemistry alone (one warp per cell): the counterparts of the
+// reference's dydt_cvode_GPU / kernel_dydt and jacobian_cvode_GPU /
+// kernel_eval_jacob (src/Integrators/Drivers/CVodeGPUDriver.cu:28-106), with
+// outputs in the reference's layout.
+template <class MT, class LinT>
+__global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParams p, double* dTdt, double* dYdt) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (cell >= p.ncells) return;
+    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    Vec<MT::NS> y;
+    load_cell<MT>(p, cell, lane, y.v);
+    const double P = p.P ? p.P[cell] : p.P_scalar;
+    const Vec<MT::NS> f = warp_rhs<MT>(P, y, &sm->chem, lane);
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < MT::N - 1) dYdt[(long long)i * p.ncells + cell] = f.v[s];
+        else if (i == MT::N - 1) dTdt[cell] = f.v[s];
+    }
+}
+
+// jac: per cell N*N column-major, reference order [T, Y_0 .. Y_{N-2}].
+template <class MT, class LinT>
+__global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParams p, double* jac) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (cell >= p.ncells) return;
+    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    auto* wg = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal) + cell;
+    Vec<MT::NS> y;
+    load_cell<MT>(p, cell, lane, y.v);
+    const double P = p.P ? p.P[cell] : p.P_scalar;
+    warp_jac<MT, LinT>(P, y, sm->A, &sm->chem, &wg->js, lane);
+    constexpr int N = MT::N;
+    double* out = jac + cell * (long long)(N * N);
+    for (int i = 0; i < N; ++i)
+        for (int j = lane; j < N; j += 32) {   // internal row i, column j
+            const int ri = (i == N - 1) ? 0 : i + 1, rj = (j == N - 1) ? 0 : j + 1;
+            out[ri + N * rj] = (double)sm->A[i * MT::LDA + j];
+        }
+}
+
+// FP64 FMA throughput probe: independent DFMA chains per thread.
+__global__ void k_fp64_peak(double* out, int iters) {
+    double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9, a4 = a0 + 4e-9,
+           a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+    const double m = 0.999999, c = 1e-9;
+#pragma unroll 1
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+            a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+        }
+    }
+    const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.0) out[0] = r;   // keep the chains live
+}
+
+// ------------------------------------------------------------------ handle
+struct b200ode_handle {
+    int mech = -1;
+    HostMech hm;
+    unsigned char* d_blob = nullptr;
+    DevMech dm;
+    b200ode_options opt;
+    int device = 0, num_sms = 0;
+    size_t cap = 0;   // cells
+    double* d_T = nullptr;
+    double* d_Y = nullptr;
+    double* d_P = nullptr;
+    int32_t* d_status = nullptr;
+    int32_t* d_cnt = nullptr;
+    unsigned long long* d_ctl = nullptr;   // [0] queue, [1..8] totals
+    void* d_wg = nullptr;                    // WarpGlobal scratch (saved Jacobians, ...)
+    size_t wg_bytes = 0;
+    unsigned char* d_rec = nullptr;          // step-form per-cell records
+    size_t rec_bytes = 0;
+    unsigned long long* h_done = nullptr;    // pinned host copy of the done counter
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int last_blocks_per_sm = 0;
+};
+
+namespace {
+
+template <class MT, class LinT>
+size_t warp_smem_bytes() { return sizeof(WarpSmem<MT, LinT>); }
+
+b200ode_status ensure_wg(b200ode_handle* h, size_t bytes) {
+    if (bytes <= h->wg_bytes) return B200ODE_OK;
+    if (h->d_wg) cudaFree(h->d_wg);
+    h->d_wg = nullptr;
+    h->wg_bytes = 0;
+    CUDA_TRY(cudaMalloc(&h->d_wg, bytes));
+    h->wg_bytes = bytes;
+    return B200ODE_OK;
+}
+
+template <class MT, class LinT>
+b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
+    using B = WarpBdf<MT, LinT>;
+    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+    auto kern = k_bdf<MT, LinT, 1>;
+    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t n = (size_t)p.ncells;
+    CUDA_TRY(cudaMemsetAsync(h->d_ctl, 0, 16 * sizeof(unsigned long long), st));
+    p.queue = h->d_ctl;
+    p.totals = h->d_ctl + 1;
+    p.done_count = h->d_ctl + 9;
+    if (h->opt.persistent) {
+        int bps = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, wpb * 32, smem));
+        if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
+        if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
+        h->last_blocks_per_sm = bps;
+        long long blocks = (long long)bps * h->num_sms;
+        blocks = std::max(1LL, std::min(blocks, (long long)((n + wpb - 1) / wpb)));
+        b200ode_status rc = ensure_wg(h, (size_t)blocks * wpb * sizeof(WarpGlobal<MT, LinT>));
+        if (rc != B200ODE_OK) return rc;
+        p.wglobal = h->d_wg;
+        p.records = nullptr;
+        p.steps = 0x7fffffff;
+        kern<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+        CUDA_TRY(cudaGetLastError());
+        *launches += 1;
+        return B200ODE_OK;
+    }
+    // one launch per BDF step: per-cell scratch and state records in HBM
+    b200ode_status rc = ensure_wg(h, n * sizeof(WarpGlobal<MT, LinT>));
+    if (rc != B200ODE_OK) return rc;
+    const size_t rb = n * B::kRecordBytes;
+    if (rb > h->rec_bytes) {
+        if (h->d_rec) cudaFree(h->d_rec);
+        h->d_rec = nullptr;
+        h->rec_bytes = 0;
+        CUDA_TRY(cudaMalloc(&h->d_rec, rb));
+        h->rec_bytes = rb;
+    }
+    if (!h->h_done) CUDA_TRY(cudaMallocHost(&h->h_done, sizeof(unsigned long long)));
+    CUDA_TRY(cudaMemsetAsync(h->d_rec, 0, rb, st));
+    p.wglobal = h->d_wg;
+    p.records = h->d_rec;
+    p.steps = 1;
+    const unsigned blocks = (unsigned)((n + wpb - 1) / wpb);
+    const int per_check = h->opt.use_graph ? 16 : 1;
+    cudaGraphExec_t gexec = nullptr;
+    if (h->opt.use_graph) {
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < per_check; ++i) kern<<<blocks, wpb * 32, smem, st>>>(p);
+        CUDA_TRY(cudaStreamEndCapture(st, &g));
+        cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(B200ODE_ERR_CUDA, "cudaGraphInstantiate");
+    }
+    // every launch finishes a cell or advances it one step: at most max_steps + 2 launches
+    const long long max_launch = (long long)h->opt.max_steps + 2;
+    rc = B200ODE_OK;
+    for (long long it = 0; it < max_launch; it += per_check) {
+        if (gexec) {
+            if (cudaGraphLaunch(gexec, st) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "cudaGraphLaunch"); break; }
+        } else {
+            kern<<<blocks, wpb * 32, smem, st>>>(p);
+        }
+        *launches += per_check;
+        if (cudaMemcpyAsync(h->h_done, p.done_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = fail(B200ODE_ERR_CUDA, std::string("step-form launch: ") + cudaGetErrorString(cudaGetLastError()));
+            break;
+        }
+        if (*h->h_done >= n) break;
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    return rc;
+}
+
+b200ode_status run(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
+    const bool fp64 = h->opt.precision == B200ODE_FP64;
+    if (h->mech == MECH_GRI30)
+        return fp64 ? launch_bdf<GriT, double>(h, p, st, launches) : launch_bdf<GriT, float>(h, p, st, launches);
+    return fp64 ? launch_bdf<H2T, double>(h, p, st, launches) : launch_bdf<H2T, float>(h, p, st, launches);
+}
+
+template <class MT, class LinT>
+b200ode_status launch_eval(b200ode_handle* h, KParams& p, double* d_dT, double* d_dY, double* d_jac,
+                           cudaStream_t st) {
+    const int wpb = 4;
+    const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+    const unsigned blocks = (unsigned)((p.ncells + wpb - 1) / wpb);
+    if (d_jac) {
+        b200ode_status rc = ensure_wg(h, (size_t)p.ncells * sizeof(WarpGlobal<MT, LinT>));
+        if (rc != B200ODE_OK) return rc;
+        p.wglobal = h->d_wg;
+        auto k = k_eval_jac<MT, LinT>;
+        CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k<<<blocks, wpb * 32, smem, st>>>(p, d_jac);
+    } else {
+        auto k = k_eval_rhs<MT, LinT>;
+        CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k<<<blocks, wpb * 32, smem, st>>>(p, d_dT, d_dY);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return B200ODE_OK;
+}
+
+b200ode_status ensure_cap(b200ode_handle* h, size_t n) {
+    if (n <= h->cap) return B200ODE_OK;
+    cudaFree(h->d_T); cudaFree(h->d_Y); cudaFree(h->d_P); cudaFree(h->d_status); cudaFree(h->d_cnt);
+    h->d_T = h->d_Y = h->d_P = nullptr; h->d_status = h->d_cnt = nullptr; h->cap = 0;
+    const size_t nsp = h->hm.nsp;
+    CUDA_TRY(cudaMalloc(&h->d_T, n * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&h->d_Y, n * nsp * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&h->d_P, n * sizeof(double)));
+    CUDA_TRY(cudaMalloc(&h->d_status, n * sizeof(int32_t)));
+    CUDA_TRY(cudaMalloc(&h->d_cnt, 7 * n * sizeof(int32_t)));
+    h->cap = n;
+    return B200ODE_OK;
+}
+
+b200ode_status check_args(const b200ode_handle* h, int64_t n, double t0, double t1) {
+    if (!h) return fail(B200ODE_ERR_INVALID, "null handle");
+    if (n < 0) return fail(B200ODE_ERR_INVALID, "n_cells < 0");
+    if (!(t1 == t1) || !(t0 == t0)) return fail(B200ODE_ERR_INVALID, "t0/t1 not finite");
+    return B200ODE_OK;
+}
+
+void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, double Ps, double* dT,
+                 double* dY, int32_t* dstat, int32_t* const* dcnt, double t0, double t1) {
+    std::memset(&p, 0, sizeof(p));
+    p.ncells = n;
+    p.P = dP;
+    p.P_scalar = Ps;
+    p.T = dT;
+    p.Y = dY;
+    p.status = dstat;
+    for (int i = 0; i < 7; ++i) p.cnt[i] = dcnt ? dcnt[i] : nullptr;
+    p.queue = h->d_ctl;
+    p.totals = h->d_ctl + 1;
+    p.done_count = h->d_ctl + 9;
+    p.prof = h->opt.profile_phases ? h->d_ctl + 10 : nullptr;
+    p.t0 = t0;
+    p.t1 = t1;
+    p.rtol = h->opt.reltol;
+    p.atol = h->opt.abstol;
+    p.max_steps = h->opt.max_steps;
+    p.max_order = h->opt.max_order;
+    p.refine = h->opt.refine;
+}
+
+b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {
+    unsigned long long t[15];
+    CUDA_TRY(cudaMemcpyAsync(t, h->d_ctl + 1, sizeof(t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < 5; ++i) s->phase_cycles[i] = h->opt.profile_phases ? (int64_t)t[9 + i] : 0;
+    s->total_nst = (int64_t)t[0]; s->total_nfe = (int64_t)t[1]; s->total_nje = (int64_t)t[2];
+    s->total_nsetups = (int64_t)t[3]; s->total_nni = (int64_t)t[4]; s->total_ncfn = (int64_t)t[5];
+    s->total_netf = (int64_t)t[6]; s->n_failed = (int64_t)t[7];
+    return B200ODE_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------- C ABI
+extern "C" {
+
+void b200ode_default_options(b200ode_options* o) {
+    if (!o) return;
+    o->reltol = 1.0e-6;
+    o->abstol = 1.0e-10;
+    o->max_steps = 10000;
+    o->max_order = 5;
+    o->precision = B200ODE_MIXED;
+    o->refine = 0;
+    o->persistent = 1;
+    o->warps_per_block = 0;
+    o->blocks_per_sm = 0;
+    o->queue_chunk = 1;
+    o->use_graph = 0;
+    o->device = -1;
+    o->profile_phases = 0;
+}
+
+const char* b200ode_last_error(void) { return g_last_error.c_str(); }
+
+const char* b200ode_version(void) { return "b200ode 0.1 (sm_100a)"; }
+
+int32_t b200ode_num_species(const b200ode_handle* h) { return h ? h->hm.nsp : -1; }
+
+b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts, b200ode_handle** out) {
+    if (!out) return fail(B200ODE_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    const int mech = mech_from_name(mech_name);
+    if (mech < 0)
+        return fail(B200ODE_ERR_MECHANISM,
+                    std::string("unknown mechanism '") + (mech_name ? mech_name : "(null)") +
+                        "' (available: gri30.yaml, h2o2.yaml)");
+    b200ode_options o;
+    b200ode_default_options(&o);
+    if (opts) o = *opts;
+    if (!(o.reltol >= 0.0) || !(o.abstol > 0.0))
+        return fail(B200ODE_ERR_INVALID, "reltol must be >= 0 and abstol > 0");
+    if (o.max_steps <= 0) o.max_steps = 500;
+    if (o.max_order < 1 || o.max_order > 5) o.max_order = 5;
+    if (o.precision != B200ODE_FP64 && o.precision != B200ODE_MIXED)
+        return fail(B200ODE_ERR_INVALID, "precision must be B200ODE_FP64 or B200ODE_MIXED");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(B200ODE_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    auto* h = new b200ode_handle();
+    h->mech = mech;
+    h->opt = o;
+    std::string err;
+    h->hm = pack_mechanism(mech == MECH_GRI30 ? GEN_TABLES(gri30, MECH_GRI30) : GEN_TABLES(h2o2, MECH_H2O2), &err);
+    if (h->hm.nsp == 0) {
+        delete h;
+        return fail(B200ODE_ERR_MECHANISM, "mechanism packing failed: " + err);
+    }
+    auto cleanup = [&](b200ode_status st) { b200ode_destroy(h); return st; };
+    if (o.device >= 0) {
+        if (cudaSetDevice(o.device) != cudaSuccess) return cleanup(fail(B200ODE_ERR_CUDA, "cudaSetDevice failed"));
+    }
+    if (cudaGetDevice(&h->device) != cudaSuccess) return cleanup(fail(B200ODE_ERR_CUDA, "cudaGetDevice failed"));
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, h->device) != cudaSuccess)
+        return cleanup(fail(B200ODE_ERR_CUDA, "cudaGetDeviceProperties failed"));
+    if (prop.major < 10)
+        return cleanup(fail(B200ODE_ERR_NO_DEVICE, std::string("device ") + prop.name + " is not sm_100 class"));
+    h->num_sms = prop.multiProcessorCount;
+    {
+        // mechanism tables: one device copy per (device, mechanism) for the
+        // process lifetime, published through the __constant__ descriptor
+        std::lock_guard<std::mutex> lk(g_tables_mu);
+        auto key = std::make_pair(h->device, mech);
+        auto it = g_tables.find(key);
+        if (it == g_tables.end()) {
+            unsigned char* blob = nullptr;
+            if (cudaMalloc(&blob, h->hm.blob.size()) != cudaSuccess)
+                return cleanup(fail(B200ODE_ERR_ALLOC, "cudaMalloc mechanism tables"));
+            if (cudaMemcpy(blob, h->hm.blob.data(), h->hm.blob.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+                return cleanup(fail(B200ODE_ERR_CUDA, "copy mechanism tables"));
+            const DevMech dm = h->hm.bind(blob);
+            if (cudaMemcpyToSymbol(c_mech, &dm, sizeof(DevMech), mech * sizeof(DevMech)) != cudaSuccess)
+                return cleanup(fail(B200ODE_ERR_CUDA, "publish mechanism descriptor"));
+            it = g_tables.emplace(key, blob).first;
+        }
+        h->d_blob = it->second;
+        h->dm = h->hm.bind(h->d_blob);
+    }
+    if (cudaMalloc(&h->d_ctl, 16 * sizeof(unsigned long long)) != cudaSuccess)
+        return cleanup(fail(B200ODE_ERR_ALLOC, "cudaMalloc control block"));
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(fail(B200ODE_ERR_CUDA, "cudaStreamCreate"));
+    for (auto& e : h->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return cleanup(fail(B200ODE_ERR_CUDA, "cudaEventCreate"));
+    *out = h;
+    return B200ODE_OK;
+}
+
+void b200ode_destroy(b200ode_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->d_T); cudaFree(h->d_Y); cudaFree(h->d_P);
+    cudaFree(h->d_status); cudaFree(h->d_cnt); cudaFree(h->d_ctl); cudaFree(h->d_wg);
+    cudaFree(h->d_rec);
+    if (h->h_done) cudaFreeHost(h->h_done);
+    for (auto& e : h->ev) if (e) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n, const double* dP, double Ps,
+                                        double* dT, double* dY, double t0, double t1, int32_t* dstat,
+                                        b200ode_stats* stats, void* stream) {
+    b200ode_status rc = check_args(h, n, t0, t1);
+    if (rc != B200ODE_OK) return rc;
+    if (n == 0) {
+        if (stats) { std::memset(stats, 0, sizeof(*stats)); }
+        return B200ODE_OK;
+    }
+    if (!dT || !dY) return fail(B200ODE_ERR_INVALID, "null T or Y");
+    cudaStream_t st = (cudaStream_t)stream;
+    int32_t* dcnt[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (stats) {
+        int32_t* src[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+        for (int i = 0; i < 7; ++i) dcnt[i] = src[i];
+    }
+    KParams p;
+    fill_params(h, p, n, dP, Ps, dT, dY, dstat, dcnt, t0, t1);
+    int launches = 0;
+    CUDA_TRY(cudaEventRecord(h->ev[1], st));
+    rc = run(h, p, st, &launches);
+    if (rc != B200ODE_OK) return rc;
+    CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    if (stats) {
+        rc = read_totals(h, stats, st);
+        if (rc != B200ODE_OK) return rc;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+        stats->kernel_ms = ms;
+        stats->h2d_ms = stats->d2h_ms = 0.0;
+        stats->gpu_launches = launches;
+    }
+    return B200ODE_OK;
+}
+
+b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n, const double* P, double Ps, double* T,
+                                 double* Y, double t0, double t1, int32_t* cell_status,
+                                 b200ode_stats* stats) {
+    b200ode_status rc = check_args(h, n, t0, t1);
+    if (rc != B200ODE_OK) return rc;
+    if (n == 0) {
+        if (stats) {
+            int32_t* keep[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+            std::memset(stats, 0, sizeof(*stats));
+            stats->nst = keep[0]; stats->nfe = keep[1]; stats->nje = keep[2]; stats->nsetups = keep[3];
+            stats->nni = keep[4]; stats->ncfn = keep[5]; stats->netf = keep[6];
+        }
+        return B200ODE_OK;
+    }
+    if (!T || !Y) return fail(B200ODE_ERR_INVALID, "null T or Y");
+    if (!P && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
+    rc = ensure_cap(h, (size_t)n);
+    if (rc != B200ODE_OK) return rc;
+    cudaStream_t st = h->stream;
+    const size_t nsp = h->hm.nsp;
+    const bool want_cnt = stats && (stats->nst || stats->nfe || stats->nje || stats->nsetups ||
+                                    stats->nni || stats->ncfn || stats->netf);
+    CUDA_TRY(cudaEventRecord(h->ev[0], st));
+    CUDA_TRY(cudaMemcpyAsync(h->d_T, T, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(h->d_Y, Y, n * nsp * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (P) CUDA_TRY(cudaMemcpyAsync(h->d_P, P, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaEventRecord(h->ev[1], st));
+    int32_t* dcnt[7];
+    for (int i = 0; i < 7; ++i) dcnt[i] = want_cnt ? h->d_cnt + (size_t)i * n : nullptr;
+    KParams p;
+    fill_params(h, p, n, P ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, h->d_status, dcnt, t0, t1);
+    int launches = 0;
+    rc = run(h, p, st, &launches);
+    if (rc != B200ODE_OK) return rc;
+    CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    CUDA_TRY(cudaMemcpyAsync(T, h->d_T, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(Y, h->d_Y, n * nsp * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (cell_status)
+        CUDA_TRY(cudaMemcpyAsync(cell_status, h->d_status, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    if (want_cnt) {
+        int32_t* dst[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+        for (int i = 0; i < 7; ++i)
+            if (dst[i])
+                CUDA_TRY(cudaMemcpyAsync(dst[i], h->d_cnt + (size_t)i * n, n * sizeof(int32_t),
+                                         cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaEventRecord(h->ev[3], st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (stats) {
+        rc = read_totals(h, stats, st);
+        if (rc != B200ODE_OK) return rc;
+        float a = 0.f, b = 0.f, c = 0.f;
+        cudaEventElapsedTime(&a, h->ev[0], h->ev[1]);
+        cudaEventElapsedTime(&b, h->ev[1], h->ev[2]);
+        cudaEventElapsedTime(&c, h->ev[2], h->ev[3]);
+        stats->h2d_ms = a;
+        stats->kernel_ms = b;
+        stats->d2h_ms = c;
+        stats->gpu_launches = launches;
+    }
+    return B200ODE_OK;
+}
+
+static b200ode_status eval_chem(b200ode_handle* h, int64_t n, const double* P, double Ps, const double* T,
+                                const double* Y, double* dTdt, double* dYdt, double* jac) {
+    b200ode_status rc = check_args(h, n, 0.0, 0.0);
+    if (rc != B200ODE_OK) return rc;
+    if (n == 0) return B200ODE_OK;
+    if (!T || !Y || (!jac && (!dTdt || !dYdt))) return fail(B200ODE_ERR_INVALID, "null buffer");
+    if (!P && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
+    rc = ensure_cap(h, (size_t)n);
+    if (rc != B200ODE_OK) return rc;
+    cudaStream_t st = h->stream;
+    const size_t N = h->hm.nsp;
+    CUDA_TRY(cudaMemcpyAsync(h->d_T, T, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(h->d_Y, Y, n * N * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (P) CUDA_TRY(cudaMemcpyAsync(h->d_P, P, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    KParams p;
+    fill_params(h, p, n, P ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, nullptr, nullptr, 0.0, 0.0);
+    double* d_out = nullptr;
+    const size_t out_elems = jac ? (size_t)n * N * N : (size_t)n * (N - 1) + n;
+    CUDA_TRY(cudaMallocAsync(&d_out, out_elems * sizeof(double), st));
+    const bool fp64 = h->opt.precision == B200ODE_FP64;
+    double* d_dT = jac ? nullptr : d_out;
+    double* d_dY = jac ? nullptr : d_out + n;
+    double* d_jac = jac ? d_out : nullptr;
+    if (h->mech == MECH_GRI30)
+        rc = fp64 ? launch_eval<GriT, double>(h, p, d_dT, d_dY, d_jac, st)
+                  : launch_eval<GriT, float>(h, p, d_dT, d_dY, d_jac, st);
+    else
+        rc = fp64 ? launch_eval<H2T, double>(h, p, d_dT, d_dY, d_jac, st)
+                  : launch_eval<H2T, float>(h, p, d_dT, d_dY, d_jac, st);
+    if (rc == B200ODE_OK) {
+        if (jac) {
+            CUDA_TRY(cudaMemcpyAsync(jac, d_out, out_elems * sizeof(double), cudaMemcpyDeviceToHost, st));
+        } else {
+            CUDA_TRY(cudaMemcpyAsync(dTdt, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(cudaMemcpyAsync(dYdt, d_out + n, n * (N - 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+    }
+    cudaFreeAsync(d_out, st);
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return rc;
+}
+
+b200ode_status b200ode_eval_rhs(b200ode_handle* h, int64_t n, const double* P, double Ps, const double* T,
+                                const double* Y, double* dTdt, double* dYdt) {
+    return eval_chem(h, n, P, Ps, T, Y, dTdt, dYdt, nullptr);
+}
+
+b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n, const double* P, double Ps,
+                                     const double* T, const double* Y, double* jac) {
+    if (!jac) return fail(B200ODE_ERR_INVALID, "null jac");
+    return eval_chem(h, n, P, Ps, T, Y, nullptr, nullptr, jac);
+}
+
+b200ode_status b200ode_fp64_peak(int32_t device, double* gflops) {
+    if (!gflops) return fail(B200ODE_ERR_INVALID, "null output");
+    if (device >= 0) CUDA_TRY(cudaSetDevice(device));
+    int dev = 0, sms = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    double* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(double)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 2048, threads = 256, blocks = sms * 8;
+    k_fp64_peak<<<blocks, threads>>>(d, 16);
+    cudaEventRecord(a);
+    k_fp64_peak<<<blocks, threads>>>(d, iters);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(B200ODE_ERR_CUDA, cudaGetErrorString(e));
+    const double flops = 2.0 * 8.0 * 16.0 * iters * (double)threads * blocks;
+    *gflops = flops / (ms * 1e-3) / 1e9;
+    return B200ODE_OK;
+}
+
+}  // extern "C"

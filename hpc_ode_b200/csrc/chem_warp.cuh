@@ -1,0 +1,494 @@
+// Warp-per-cell chemistry: constant-pressure RHS and analytic Jacobian.
+//
+// One warp evaluates one cell.  The 32 lanes split the work three ways:
+//   * species phase   -- lane l owns species l and l+32 (thermo, concentrations);
+//   * reaction phase  -- lane l evaluates reaction slot 32*g + l of group g
+//                        (kf, Kc, third-body / falloff modifiers, rates of progress);
+//   * gather phase    -- production rates summed from the rates of progress with
+//                        a balanced, coalesced (species, reaction) list: every lane
+//                        sums ~1/32 of the pairs in a fixed order, partial sums
+//                        are combined per species in a fixed order (no atomics,
+//                        so results do not depend on scheduling).
+// Per-cell intermediates (concentrations, -g/RT, rates) live in shared memory,
+// never in HBM (the reference's GPU path keeps ~31.8 KB of them per cell in global
+// memory: src/Mechanism/GPU/gpu_memory.cu:3-37).
+//
+// Reference math (pyJac C, src/Mechanism/CPU): eval_conc chem_utils.c:4-97,
+// eval_rxn_rates rxn_rates.c:2-3862, get_rxn_pres_mod rxn_rates_pres_mod.c:5-366,
+// eval_spec_rates spec_rates.c:4, dydt dydt.c:7-133, eval_jacob jacob.c:3-372.
+//
+// Internal element order of a state vector: element i < N-1 is Y_i, element N-1
+// is T (so that a lane's species slot and state slot coincide); the reference's
+// order is [T, Y_0 .. Y_{N-2}].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "mech_dev.h"
+
+namespace b200 {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr double kRU = 8314.4621;
+
+template <int N_, int NR_, int ID_>
+struct MechT {
+    static constexpr int ID = ID_;                            // index into c_mech
+    static constexpr int N = N_;                              // state length == species count
+    static constexpr int NS = (N_ + 31) / 32;                 // elements per lane
+    static constexpr int NSLOT = ((NR_ + 32) / 32) * 32;      // reaction slots (>= 1 padding slot)
+    static constexpr int NG = NSLOT / 32;                     // reaction groups
+    static constexpr int LDA = (N_ % 2 == 0) ? N_ + 1 : N_;   // odd stride: conflict-free rows/cols
+    static constexpr int NUNITMAX = N_ + (6 * NSLOT) / kGatherUnit + 1;   // gather units bound
+};
+
+// Mechanism descriptors (one per compiled mechanism), set once per device.
+__constant__ DevMech c_mech[2];
+
+template <class MT>
+__device__ __forceinline__ const DevMech& mech() { return c_mech[MT::ID]; }
+
+// A lane's slice of a state vector (element i = lane + 32*s), passed by value
+// so the heavy phases can be single-copy (non-inlined) functions without
+// forcing the caller's state into local memory.
+template <int NS>
+struct Vec {
+    double v[NS];
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+
+// Per-warp shared scratch of the chemistry.
+template <class MT>
+struct ChemSmem {
+    double C[MT::N + 1];          // concentrations [kmol/m^3]; C[N] = 1 (padding factor)
+    double G[MT::N + 1];          // s/R - h/RT; G[N] = 0
+    double H[MT::N + 1];          // h/RT; H[N] = 0
+    double q[MT::NSLOT];          // rates of progress (Jacobian: reused for per-species work)
+    double part[MT::NUNITMAX];    // gather partial sums
+};
+
+// Per-warp global scratch of the Jacobian (L1/L2 resident; the Jacobian is rare).
+template <class MT>
+struct JacScratch {
+    double dqdT[MT::NSLOT];       // d q / d T at fixed mass fractions
+    double sr[MT::NSLOT];         // sum_i (d q / d C_i) C_i
+};
+
+// NASA-7 polynomials of species k at T: cp/R, h/RT, s/R - h/RT, d(cp/R)/dT.
+__device__ __forceinline__ void nasa7(const DevMech& M, int k, double T, double logT, double invT,
+                                      double& cpR, double& hRT, double& mgRT, double& dcpR) {
+    const double* a = M.nasa + 14 * k + ((T <= __ldg(M.tmid + k)) ? 0 : 7);
+    const double a0 = __ldg(a + 0), a1 = __ldg(a + 1), a2 = __ldg(a + 2), a3 = __ldg(a + 3),
+                 a4 = __ldg(a + 4), a5 = __ldg(a + 5), a6 = __ldg(a + 6);
+    cpR = a0 + T * (a1 + T * (a2 + T * (a3 + a4 * T)));
+    hRT = a0 + T * (a1 * 0.5 + T * (a2 * (1.0 / 3.0) + T * (a3 * 0.25 + a4 * 0.2 * T))) + a5 * invT;
+    mgRT = a0 * (logT - 1.0) + T * (a1 * 0.5 + T * (a2 * (1.0 / 6.0) + T * (a3 * (1.0 / 12.0) + a4 * 0.05 * T)))
+           - a5 * invT + a6;
+    dcpR = a1 + T * (2.0 * a2 + T * (3.0 * a3 + 4.0 * a4 * T));
+}
+
+// Common cell quantities of one RHS / Jacobian evaluation.
+struct CellThermo {
+    double T, logT, invT, m, rho, mw_avg, yN, mC;   // mC = m - sum_k C_k
+};
+
+// Species phase: concentrations and Gibbs terms into shared memory.
+template <class MT>
+__device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, const double (&y)[MT::NS],
+                                                    ChemSmem<MT>* sm, int lane, double (&Yk)[MT::NS],
+                                                    double (&cpR)[MT::NS], double (&hRT)[MT::NS],
+                                                    double (&dcpR)[MT::NS]) {
+    constexpr int N = MT::N;
+    CellThermo c;
+    c.T = __shfl_sync(kFull, y[(N - 1) / 32], (N - 1) % 32);
+    double sy = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) sy += y[s];
+    }
+    c.yN = 1.0 - warp_sum(sy);
+    double sw = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        Yk[s] = (i < N - 1) ? y[s] : ((i == N - 1) ? c.yN : 0.0);
+        if (i < N) sw += Yk[s] * __ldg(M.inv_mw + i);
+    }
+    c.mw_avg = 1.0 / warp_sum(sw);
+    c.logT = log(c.T);
+    c.invT = 1.0 / c.T;
+    c.rho = P * c.mw_avg / (kRU * c.T);
+    c.m = P / (kRU * c.T);
+    double csum = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N) {
+            double g;
+            nasa7(M, i, c.T, c.logT, c.invT, cpR[s], hRT[s], g, dcpR[s]);
+            const double Ci = c.rho * Yk[s] * __ldg(M.inv_mw + i);
+            csum += Ci;
+            sm->C[i] = Ci;
+            sm->G[i] = g;
+            sm->H[i] = hRT[s];
+        } else {
+            cpR[s] = hRT[s] = dcpR[s] = 0.0;
+        }
+    }
+    c.mC = c.m - warp_sum(csum);
+    if (lane == 0) {
+        sm->C[N] = 1.0;
+        sm->G[N] = 0.0;
+        sm->H[N] = 0.0;
+    }
+    __syncwarp();
+    return c;
+}
+
+// Rates of one reaction slot.  With Deriv, also the pieces of its derivative.
+struct RxnOut {
+    double q;            // (Rf - Rr) * phi
+    double kf, kr;       // rate coefficients
+    double Rf, Rr;       // kf prod C', kr prod C''
+    double phi, thd, dphi_dthd, dphi_dT, dlnkf_dT;
+};
+
+template <bool Deriv>
+__device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int s, const CellThermo& c,
+                                           const double* C, const double* G) {
+    RxnOut o;
+    o.q = 0.0; o.kf = 0.0; o.kr = 0.0; o.Rf = 0.0; o.Rr = 0.0; o.phi = 1.0; o.thd = 0.0;
+    o.dphi_dthd = 0.0; o.dphi_dT = 0.0; o.dlnkf_dT = 0.0;
+    const int fl = __ldg(M.flags + s);
+    if (!(fl & kFlagActive)) return o;
+    const int ns = M.nslot;
+    const int r0 = __ldg(M.rf + s), r1 = __ldg(M.rf + ns + s), r2 = __ldg(M.rf + 2 * ns + s);
+    const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
+    const double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
+    const double kf = (fl & kFlagConstK) ? __ldg(M.Aconst + s) : exp(lkf);
+    o.kf = kf;
+    o.Rf = kf * ((C[r0] * C[r1]) * C[r2]);
+    if (Deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
+    if (fl & kFlagRev) {
+        const int p0 = __ldg(M.pf + s), p1 = __ldg(M.pf + ns + s), p2 = __ldg(M.pf + 2 * ns + s);
+        const int dnu = __ldg(M.dnu + s);
+        const double sg = (G[p0] + G[p1] + G[p2]) - (G[r0] + G[r1] + G[r2]);
+        const double lnKc = sg - dnu * c.logT + __ldg(M.lnPfac + s);
+        const double kr = (fl & kFlagConstK) ? __ldg(M.Aconst + s) * exp(-lnKc) : exp(lkf - lnKc);
+        o.kr = kr;
+        o.Rr = kr * ((C[p0] * C[p1]) * C[p2]);
+    }
+    const int type = fl & kFlagTypeMask;
+    if (type != 0) {
+        double thd;
+        if (fl & kFlagCatalyst) {
+            thd = c.mC + C[__ldg(M.cat_sp + s)];   // m - sum_{k != s} C_k
+        } else {
+            thd = c.m;
+            const int off = __ldg(M.tb_off + s), len = __ldg(M.tb_len + s);
+            for (int t = 0; t < len; ++t) thd += __ldg(M.tb_alpha + off + t) * C[__ldg(M.tb_sp + off + t)];
+        }
+        o.thd = thd;
+        if (type == 1) {
+            o.phi = thd;
+            o.dphi_dthd = 1.0;
+        } else {
+            const double b0 = __ldg(M.b0 + s), EaR0 = __ldg(M.EaR0 + s);
+            const double k0 = (fl & kFlagConstK0) ? __ldg(M.A0const + s)
+                                                  : exp(__ldg(M.logA0 + s) + b0 * c.logT - EaR0 * c.invT);
+            const double Pr = k0 * thd / kf;
+            double F = 1.0, dl_dx = 0.0, dl_dT = 0.0;
+            if (type == 3) {
+                const double a = __ldg(M.troe_a + s), iT3 = __ldg(M.troe_iT3 + s), iT1 = __ldg(M.troe_iT1 + s);
+                const double e3 = exp(-c.T * iT3), e1 = exp(-c.T * iT1);
+                double Fcent = (1.0 - a) * e3 + a * e1;
+                double dFcent = 0.0;
+                if (Deriv) dFcent = -(1.0 - a) * iT3 * e3 - a * iT1 * e1;
+                if (fl & kFlagT2) {
+                    const double T2 = __ldg(M.troe_T2 + s);
+                    const double e2 = exp(-T2 * c.invT);
+                    Fcent += e2;
+                    if (Deriv) dFcent += T2 * c.invT * c.invT * e2;
+                }
+                const double Fc = log10(fmax(Fcent, 1.0e-300));
+                const double x = log10(fmax(Pr, 1.0e-300));
+                const double A = x - 0.67 * Fc - 0.4;
+                const double B = 0.806 - 1.1762 * Fc - 0.14 * x;
+                const double u = A / B;
+                const double den = 1.0 + u * u;
+                F = exp10(Fc / den);
+                if (Deriv) {
+                    const double du_dx = (B + 0.14 * A) / (B * B);
+                    const double du_dFc = (-0.67 * B + 1.1762 * A) / (B * B);
+                    dl_dx = (Pr > 1.0e-300) ? -Fc * 2.0 * u * du_dx / (den * den) : 0.0;
+                    const double dl_dFc = 1.0 / den - Fc * 2.0 * u * du_dFc / (den * den);
+                    const double dFc_dT = (Fcent > 1.0e-300) ? dFcent / (Fcent * 2.302585092994046) : 0.0;
+                    dl_dT = dl_dFc * dFc_dT;
+                }
+            }
+            const double blend = Pr / (1.0 + Pr);
+            o.phi = F * blend;
+            if (Deriv) {
+                const double dphi_dPr = F / ((1.0 + Pr) * (1.0 + Pr)) + F / (1.0 + Pr) * dl_dx;
+                o.dphi_dthd = dphi_dPr * (k0 / kf);
+                const double dlnPr_dT = (b0 + EaR0 * c.invT) * c.invT - (b + EaR * c.invT) * c.invT;
+                o.dphi_dT = dphi_dPr * Pr * dlnPr_dT + blend * F * 2.302585092994046 * dl_dT;
+            }
+        }
+    }
+    o.q = (o.Rf - o.Rr) * o.phi;
+    return o;
+}
+
+// Balanced gather: out[s] = sum over species (lane + 32 s)'s (slot, nu) pairs of
+// nu * src[slot].  Unit partial sums go through sm->part.
+template <class MT>
+__device__ __forceinline__ void gather(const DevMech& M, const double* src, ChemSmem<MT>* sm, int lane,
+                                       double (&out)[MT::NS]) {
+    double acc = 0.0;
+    const int gmax = M.gmax;
+    const int* gw = M.gword + lane;
+#pragma unroll 4
+    for (int e = 0; e < gmax; ++e) {
+        const int w = __ldg(gw + 32 * e);
+        acc += (double)(((w >> 11) & 31) - 16) * src[w & 2047];
+        if (w & (1 << 16)) {
+            sm->part[w >> 17] = acc;
+            acc = 0.0;
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        double v = 0.0;
+        if (i < MT::N) {
+            const int u0 = __ldg(M.unit_off + i), u1 = __ldg(M.unit_off + i + 1);
+            for (int u = u0; u < u1; ++u) v += sm->part[u];
+        }
+        out[s] = v;
+    }
+    __syncwarp();
+}
+
+// f = dy/dt for the warp's cell.  y, f: lane elements in internal order.
+template <class MT>
+__device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, ChemSmem<MT>* sm, int lane) {
+    constexpr int N = MT::N;
+    const DevMech& M = mech<MT>();
+    double y[MT::NS];
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) y[s] = yv.v[s];
+    double Yk[MT::NS], cpR[MT::NS], hRT[MT::NS], dcpR[MT::NS];
+    const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
+#pragma unroll 1
+    for (int g = 0; g < MT::NG; ++g) {
+        const int s = 32 * g + lane;
+        sm->q[s] = rxn_eval<false>(M, s, c, sm->C, sm->G).q;
+    }
+    __syncwarp();
+    double om[MT::NS];
+    gather<MT>(M, sm->q, sm, lane, om);
+    double qsum = 0.0, cpsum = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N) {
+            qsum += om[s] * hRT[s];
+            cpsum += cpR[s] * Yk[s] * __ldg(M.inv_mw + i);
+        }
+    }
+    const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k h_k W_k   [W/m^3]
+    const double cp_avg = kRU * warp_sum(cpsum);           // [J/kg/K]
+    const double dTdt = -Q / (c.rho * cp_avg);
+    Vec<MT::NS> fv;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) fv.v[s] = om[s] * (__ldg(M.mw + i) / c.rho);
+        else if (i == N - 1) fv.v[s] = dTdt;
+        else fv.v[s] = 0.0;
+    }
+    __syncwarp();   // shared scratch is reused by the next evaluation
+    return fv;
+}
+
+// Analytic Jacobian J = d f / d y (internal order) into A (row-major, lda MT::LDA),
+// in precision LinT.  Chain rule through concentrations and the closure species:
+//   dC_i/dY_j = rho/W_i (delta_ij - delta_{i,N-1}) - C_i Wbar (1/W_j - 1/W_{N-1}).
+// d q / d C_j is scattered into the species-space rows with shared-memory
+// atomics (one warp per cell, so the accumulation never leaves the warp).
+template <class MT, class LinT>
+__device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, LinT* A, ChemSmem<MT>* sm,
+                                      JacScratch<MT>* js, int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    const DevMech& M = mech<MT>();
+    double y[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) y[s] = yv.v[s];
+    double Yk[NS], cpR[NS], hRT[NS], dcpR[NS];
+    for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
+    const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
+    const int ns = M.nslot;
+#pragma unroll 1
+    for (int g = 0; g < MT::NG; ++g) {
+        const int s = 32 * g + lane;
+        const RxnOut o = rxn_eval<true>(M, s, c, sm->C, sm->G);
+        const int fl = __ldg(M.flags + s);
+        double dqdT = 0.0, sr = 0.0, thd_term = 0.0;
+        double dRf[3] = {0.0, 0.0, 0.0}, dRr[3] = {0.0, 0.0, 0.0};
+        int rf[3], pf[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            rf[a] = __ldg(M.rf + a * ns + s);
+            pf[a] = __ldg(M.pf + a * ns + s);
+        }
+        if (fl & kFlagActive) {
+            // d ln kr / dT = d ln kf / dT - (sum nu h/RT - dnu) / T
+            double dlnkr = 0.0;
+            if (fl & kFlagRev) {
+                double dH = 0.0;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) {
+                    const int k = __ldg(M.jrow + e * ns + s);
+                    if (k >= 0) dH += (double)__ldg(M.jnu + e * ns + s) * sm->H[k];
+                }
+                dlnkr = o.dlnkf_dT - (dH - (double)__ldg(M.dnu + s)) * c.invT;
+            }
+            const double R = o.Rf - o.Rr;
+            const double dR_dT = o.Rf * o.dlnkf_dT - o.Rr * dlnkr;
+            int ordf = 0, ordr = 0;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) { ordf += (rf[a] < N); ordr += (pf[a] < N); }
+            const double Sr = o.phi * (ordf * o.Rf - ordr * o.Rr);
+            thd_term = R * o.dphi_dthd;
+            dqdT = o.phi * dR_dT + R * o.dphi_dT - (Sr + thd_term * o.thd) * c.invT;
+            sr = Sr + thd_term * (o.thd - c.m);
+            const double* C = sm->C;
+            dRf[0] = o.phi * o.kf * (C[rf[1]] * C[rf[2]]);
+            dRf[1] = o.phi * o.kf * (C[rf[0]] * C[rf[2]]);
+            dRf[2] = o.phi * o.kf * (C[rf[0]] * C[rf[1]]);
+            dRr[0] = o.phi * o.kr * (C[pf[1]] * C[pf[2]]);
+            dRr[1] = o.phi * o.kr * (C[pf[0]] * C[pf[2]]);
+            dRr[2] = o.phi * o.kr * (C[pf[0]] * C[pf[1]]);
+        }
+        sm->q[s] = o.q;
+        js->dqdT[s] = dqdT;
+        js->sr[s] = sr;
+        if (fl & kFlagActive) {
+            const int off = __ldg(M.tb_off + s), len = __ldg(M.tb_len + s);
+            const int cat = (fl & kFlagCatalyst) ? __ldg(M.cat_sp + s) : -1;
+#pragma unroll 1
+            for (int e = 0; e < 6; ++e) {
+                const int k = __ldg(M.jrow + e * ns + s);
+                if (k < 0) break;
+                const double nu = (double)__ldg(M.jnu + e * ns + s);
+                LinT* row = A + k * LDA;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    if (rf[a] < N) atomicAdd(row + rf[a], (LinT)(nu * dRf[a]));
+                    if (pf[a] < N) atomicAdd(row + pf[a], (LinT)(-nu * dRr[a]));
+                }
+                const double tt = nu * thd_term;
+                if (cat >= 0) {
+                    // [M] = m - sum_{k != cat} C_k: d[M]/dC_j = -1 for j != cat
+                    for (int j = 0; j < N; ++j)
+                        if (j != cat) atomicAdd(row + j, (LinT)(-tt));
+                } else {
+                    for (int t = 0; t < len; ++t)
+                        atomicAdd(row + __ldg(M.tb_sp + off + t), (LinT)(tt * __ldg(M.tb_alpha + off + t)));
+                }
+            }
+        }
+    }
+    __syncwarp();
+    // per-species totals (fixed-order gathers)
+    double w[NS], dw[NS], sk[NS];
+    gather<MT>(M, sm->q, sm, lane, w);
+    gather<MT>(M, js->dqdT, sm, lane, dw);
+    gather<MT>(M, js->sr, sm, lane, sk);
+    double* spw = sm->q;   // per-species work reuses the rate buffer: [3][N]
+    const double WN = __ldg(M.mw + N - 1);
+    double dfdT[NS];
+    double qsum = 0.0, cpsum = 0.0, Ssum2 = 0.0, Ssum3 = 0.0, accTT = 0.0, dcpsum = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        dfdT[s] = 0.0;
+        if (i < N) {
+            const double Wi = __ldg(M.mw + i);
+            const double fk = w[s] * Wi / c.rho;
+            dfdT[s] = (Wi / c.rho) * (dw[s] + w[s] * c.invT);
+            const double hk = kRU * c.T * hRT[s] / Wi;     // J/kg
+            const double cpk = kRU * cpR[s] / Wi;          // J/kg/K
+            const double X = (c.mw_avg / c.rho) * (w[s] - sk[s]);
+            spw[0 * N + i] = hk * Wi;                      // h_k W_k
+            spw[1 * N + i] = cpk;
+            spw[2 * N + i] = X;
+            qsum += hk * fk;
+            cpsum += cpk * Yk[s];
+            Ssum2 += hk * Wi * (double)A[i * LDA + (N - 1)];
+            Ssum3 += hk * Wi * X;
+            accTT += cpk * fk + hk * dfdT[s];
+            dcpsum += Yk[s] * kRU * dcpR[s] / Wi;
+        }
+    }
+    const double cp_avg = warp_sum(cpsum);
+    const double fT = -warp_sum(qsum) / cp_avg;
+    const double S2 = warp_sum(Ssum2);
+    const double S3 = warp_sum(Ssum3);
+    const double JTT = -(warp_sum(accTT) + fT * warp_sum(dcpsum)) / cp_avg;
+    __syncwarp();
+    // T row (state row N-1): lane owns columns j < N-1
+    double trow[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int j = lane + 32 * s;
+        trow[s] = 0.0;
+        if (j < N - 1) {
+            double S1 = 0.0;
+            for (int k = 0; k < N; ++k) S1 += spw[k] * (double)A[k * LDA + j];
+            const double Wj = __ldg(M.mw + j);
+            const double dj = 1.0 / Wj - 1.0 / WN;
+            trow[s] = -(S1 / Wj - S2 / WN + dj * S3 + fT * (spw[N + j] - spw[N + N - 1])) / cp_avg;
+        }
+    }
+    __syncwarp();
+    // species rows k < N-1 (lane owns rows), then the T column
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int k = lane + 32 * s;
+        if (k < N - 1) {
+            LinT* row = A + k * LDA;
+            const double Wk = __ldg(M.mw + k);
+            const double cN = (double)row[N - 1] / WN;
+            const double X = spw[2 * N + k];
+            for (int j = 0; j < N - 1; ++j) {
+                const double iWj = __ldg(M.inv_mw + j);
+                row[j] = (LinT)(Wk * ((double)row[j] * iWj - cN + X * (iWj - 1.0 / WN)));
+            }
+            row[N - 1] = (LinT)dfdT[s];
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int j = lane + 32 * s;
+        if (j < N - 1) A[(N - 1) * LDA + j] = (LinT)trow[s];
+    }
+    if (lane == 0) A[(N - 1) * LDA + (N - 1)] = (LinT)JTT;
+    __syncwarp();
+}
+
+}  // namespace b200

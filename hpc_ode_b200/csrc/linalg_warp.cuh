@@ -1,0 +1,133 @@
+// Warp-per-cell dense LU with partial pivoting and triangular solves for the
+// Newton matrix M = I - gamma*J of one cell (N x N, N = 53 for GRI-Mech 3.0).
+//
+// Replaces, for one cell, MAGMA's batched getrf/getrs behind SUNDIALS'
+// SUNLinSol_MagmaDense (ext/magma-2.6.2/src/dgetrf_batched.cpp:82-230,
+// dgetrs_batched.cpp:87-190; used at src/Integrators/CVodeIntegratorGPU.cpp:86-90)
+// and SUNDIALS' serial dense getrf/getrs on the CPU path
+// (SUNLinSol_Dense, CVodeIntegrator.cpp:127-131).  Same factorization: row
+// interchanges chosen as the first index of the largest |a_ik| in column k,
+// multipliers scaled by the reciprocal of the pivot, unit-lower L and upper U
+// stored in place.
+//
+// Layout: A row-major in shared memory with an odd leading dimension, so
+// that 32 lanes reading one column (different rows) or one row (different
+// columns) hit 32 distinct banks.  The matrix type LinT is float in the
+// mixed-precision form and double in the FP64 form; right-hand sides arrive
+// and leave in FP64.
+#pragma once
+
+#include "chem_warp.cuh"
+
+namespace b200 {
+
+template <class T>
+__device__ __forceinline__ T absT(T v) { return v < T(0) ? -v : v; }
+
+// Factor A in place.  piv[k] = row swapped with row k at step k; perm = the
+// composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
+// Returns 0, or k+1 if U_kk == 0 (singular).  All 32 lanes call it.
+template <class MT, class LinT>
+__device__ __noinline__ int warp_lu(LinT* A, int* perm, LinT* dinv, int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA;
+    int sing = 0;
+    int pv = lane;   // lane i tracks perm[i] for i = lane, lane + 32
+    int pv2 = lane + 32;
+#pragma unroll 1
+    for (int k = 0; k < N; ++k) {
+        // pivot: first index of the max |a_ik|, i >= k
+        LinT best = LinT(-1);
+        int bi = N;
+        for (int i = k + lane; i < N; i += 32) {
+            const LinT v = absT(A[i * LDA + k]);
+            if (v > best) { best = v; bi = i; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const LinT ov = __shfl_xor_sync(kFull, best, o);
+            const int oi = __shfl_xor_sync(kFull, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
+        if (bi != k) {
+            for (int j = lane; j < N; j += 32) {
+                const LinT t = A[k * LDA + j];
+                A[k * LDA + j] = A[bi * LDA + j];
+                A[bi * LDA + j] = t;
+            }
+            // compose the permutation: swap entries k and bi
+            const int ok = __shfl_sync(kFull, (k < 32) ? pv : pv2, k & 31);
+            const int ob = __shfl_sync(kFull, (bi < 32) ? pv : pv2, bi & 31);
+            if (lane == (k & 31)) { if (k < 32) pv = ob; else pv2 = ob; }
+            if (lane == (bi & 31)) { if (bi < 32) pv = ok; else pv2 = ok; }
+            __syncwarp();
+        }
+        const LinT inv = LinT(1) / A[k * LDA + k];
+        if (lane == 0) dinv[k] = inv;
+        for (int i = k + 1 + lane; i < N; i += 32) A[i * LDA + k] *= inv;
+        __syncwarp();
+        // rank-1 update of the trailing block; lane owns columns j
+        for (int j = k + 1 + lane; j < N; j += 32) {
+            const LinT ukj = A[k * LDA + j];
+            if (ukj != LinT(0)) {
+#pragma unroll 4
+                for (int i = k + 1; i < N; ++i) A[i * LDA + j] -= A[i * LDA + k] * ukj;
+            }
+        }
+        __syncwarp();
+    }
+    if (lane < N) perm[lane] = pv;
+    if (lane + 32 < N) perm[lane + 32] = pv2;
+    __syncwarp();
+    return sing;
+}
+
+// Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + 32 s) in,
+// solution out.  Arithmetic in LinT.
+template <class MT, class LinT>
+__device__ __noinline__ Vec<MT::NS> warp_lu_solve(const LinT* A, const int* perm, const LinT* dinv,
+                                                  const Vec<MT::NS> bv, int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    const double (&b)[NS] = bv.v;
+    Vec<NS> out;
+    LinT x[NS];
+    // gather: x[i] = b[perm[i]]
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        const int src = (i < N) ? perm[i] : i;
+        double v = 0.0;
+#pragma unroll
+        for (int s2 = 0; s2 < NS; ++s2) {
+            const double t = __shfl_sync(kFull, b[s2], src & 31);
+            if ((src >> 5) == s2) v = t;
+        }
+        x[s] = (i < N) ? (LinT)v : LinT(0);
+    }
+    // forward: unit lower
+#pragma unroll
+    for (int k = 0; k < N - 1; ++k) {
+        const LinT xk = __shfl_sync(kFull, x[k >> 5], k & 31);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int i = lane + 32 * s;
+            if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
+        }
+    }
+    // backward: upper
+#pragma unroll
+    for (int k = N - 1; k >= 0; --k) {
+        const LinT xk = __shfl_sync(kFull, x[k >> 5], k & 31) * dinv[k];
+        if (lane == (k & 31)) x[k >> 5] = xk;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int i = lane + 32 * s;
+            if (i < k) x[s] -= A[i * LDA + k] * xk;
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) out.v[s] = (double)x[s];
+    return out;
+}
+
+}  // namespace b200

@@ -1,0 +1,359 @@
+// Device-side mechanism description and its host packing.
+//
+// The generated tables (csrc/mech/<name>_mech.h, written by
+// hpc_ode_b200/mechanism.py with the pyJac conventions of the reference's
+// src/Mechanism/CPU kernels) are repacked on the host into the layout the warp
+// kernels read:
+//   * species arrays (molecular weights, NASA-7 coefficients), index k;
+//   * reaction "slots": reactions sorted by kind (elementary, third-body,
+//     catalyst third-body, Lindemann, Troe) and padded to groups of 32 so that
+//     the 32 lanes of a warp evaluate 32 reactions of one kind with the same
+//     instruction stream.  Every field is a separate array indexed by slot,
+//     so one group's load is one coalesced 32-wide access;
+//   * a species-major gather list (slot, net stoichiometry) so that each lane
+//     sums the production rate of its own species in a fixed order (no
+//     atomics: results do not depend on scheduling).
+#pragma once
+
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace b200 {
+
+constexpr int kFlagTypeMask = 3;     // 0 elementary, 1 third-body, 2 Lindemann, 3 Troe
+constexpr int kFlagRev = 1 << 2;     // reversible
+constexpr int kFlagConstK = 1 << 3;  // kf = A (b = 0, Ea = 0)
+constexpr int kFlagActive = 1 << 4;  // real reaction (0 for padding slots)
+constexpr int kFlagT2 = 1 << 5;      // Troe with T2 term
+constexpr int kFlagConstK0 = 1 << 6; // k0 = A0
+constexpr int kFlagCatalyst = 1 << 7;  // third body is one species s: [M] = m - sum(C) + C_s
+
+// Balanced species gather: the (species, reaction) pairs are cut into units of
+// at most kGatherUnit entries, and units are dealt to the 32 lanes so each lane
+// sums about the same number of entries.  Entry word (int32):
+//   bits 0-10  reaction slot            bits 11-15 net stoichiometry + 16
+//   bit  16    last entry of its unit   bits 17-31 unit index
+constexpr int kGatherUnit = 24;
+
+// Pointers into one device allocation (all arrays contiguous).
+struct DevMech {
+    int nsp, nrxn, nslot, ntb, nent;
+    const double* mw;       // [nsp]
+    const double* inv_mw;   // [nsp]
+    const double* tmid;     // [nsp]
+    const double* nasa;     // [nsp][14]: low range a0..a6, high range a0..a6
+    // reaction slots [nslot]
+    const double* logA;
+    const double* b;
+    const double* EaR;
+    const double* Aconst;
+    const double* lnPfac;   // dnu * ln(Patm / R)
+    const double* logA0;
+    const double* b0;
+    const double* EaR0;
+    const double* A0const;
+    const double* troe_a;
+    const double* troe_iT3;
+    const double* troe_iT1;
+    const double* troe_T2;
+    const int* flags;
+    const int* rf;          // [3][nslot] reactant factor species (nsp = dummy: C = 1, G = 0)
+    const int* pf;          // [3][nslot] product factor species
+    const int* dnu;         // [nslot]
+    const int* tb_off;      // [nslot]
+    const int* tb_len;      // [nslot]
+    const int* tb_sp;       // [ntb]
+    const double* tb_alpha; // [ntb]
+    const int* jrow;        // [6][nslot] species with nonzero net stoichiometry (-1 = none)
+    const int* jnu;         // [6][nslot] their net stoichiometric coefficient
+    const int* sp_off;      // [nsp + 1]
+    const int* sp_slot;     // [nent]
+    const int* sp_nu;       // [nent]
+    const int* cat_sp;      // [nslot] catalyst species (or -1)
+    int gmax;               // entries per lane in the balanced gather
+    int nunit;              // gather units
+    const int* gword;       // [gmax][32] entry words, lane innermost (coalesced)
+    const int* unit_off;    // [nsp + 1] units of each species (contiguous, in order)
+};
+
+// Host image of DevMech: one byte buffer plus offsets, copied to the device once.
+struct HostMech {
+    std::string name;
+    int nsp = 0, nrxn = 0, nslot = 0, ntb = 0, nent = 0;
+    std::vector<std::string> species;
+    std::vector<double> mw;
+    std::vector<int> slot_rxn;   // slot -> original reaction index (-1 = padding)
+    std::vector<unsigned char> blob;
+    // byte offsets of each array inside blob
+    size_t o_mw, o_inv_mw, o_tmid, o_nasa, o_logA, o_b, o_EaR, o_Aconst, o_lnPfac, o_logA0, o_b0,
+        o_EaR0, o_A0const, o_troe_a, o_troe_iT3, o_troe_iT1, o_troe_T2, o_flags, o_rf, o_pf,
+        o_dnu, o_tb_off, o_tb_len, o_tb_sp, o_tb_alpha, o_jrow, o_jnu, o_sp_off, o_sp_slot,
+        o_sp_nu, o_cat_sp, o_gword, o_unit_off;
+    int gmax = 0, nunit = 0;
+
+    DevMech bind(const unsigned char* base) const {
+        DevMech d;
+        d.nsp = nsp; d.nrxn = nrxn; d.nslot = nslot; d.ntb = ntb; d.nent = nent;
+        d.mw = (const double*)(base + o_mw);
+        d.inv_mw = (const double*)(base + o_inv_mw);
+        d.tmid = (const double*)(base + o_tmid);
+        d.nasa = (const double*)(base + o_nasa);
+        d.logA = (const double*)(base + o_logA);
+        d.b = (const double*)(base + o_b);
+        d.EaR = (const double*)(base + o_EaR);
+        d.Aconst = (const double*)(base + o_Aconst);
+        d.lnPfac = (const double*)(base + o_lnPfac);
+        d.logA0 = (const double*)(base + o_logA0);
+        d.b0 = (const double*)(base + o_b0);
+        d.EaR0 = (const double*)(base + o_EaR0);
+        d.A0const = (const double*)(base + o_A0const);
+        d.troe_a = (const double*)(base + o_troe_a);
+        d.troe_iT3 = (const double*)(base + o_troe_iT3);
+        d.troe_iT1 = (const double*)(base + o_troe_iT1);
+        d.troe_T2 = (const double*)(base + o_troe_T2);
+        d.flags = (const int*)(base + o_flags);
+        d.rf = (const int*)(base + o_rf);
+        d.pf = (const int*)(base + o_pf);
+        d.dnu = (const int*)(base + o_dnu);
+        d.tb_off = (const int*)(base + o_tb_off);
+        d.tb_len = (const int*)(base + o_tb_len);
+        d.tb_sp = (const int*)(base + o_tb_sp);
+        d.tb_alpha = (const double*)(base + o_tb_alpha);
+        d.jrow = (const int*)(base + o_jrow);
+        d.jnu = (const int*)(base + o_jnu);
+        d.sp_off = (const int*)(base + o_sp_off);
+        d.sp_slot = (const int*)(base + o_sp_slot);
+        d.sp_nu = (const int*)(base + o_sp_nu);
+        d.cat_sp = (const int*)(base + o_cat_sp);
+        d.gmax = gmax;
+        d.nunit = nunit;
+        d.gword = (const int*)(base + o_gword);
+        d.unit_off = (const int*)(base + o_unit_off);
+        return d;
+    }
+};
+
+// Raw generated tables of one mechanism (pointers to the static arrays).
+struct GenTables {
+    const char* name;
+    int nsp, nrxn, maxp, ntb;
+    const char* const* species_names;
+    const double *mw, *tmid, *nasa_lo, *nasa_hi;
+    const int *type, *rev;
+    const double *A, *logA, *b, *EaR, *A0, *logA0, *b0, *EaR0, *troe;
+    const int *troeT2, *reac_sp, *reac_nu, *prod_sp, *prod_nu, *tb_off, *tb_sp;
+    const double* tb_alpha;
+};
+
+// Build the packed image.  Returns an empty name on failure (message in err).
+inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
+    HostMech h;
+    const int n = g.nsp, nr = g.nrxn, P = g.maxp;
+    h.name = g.name;
+    h.nsp = n;
+    h.nrxn = nr;
+    for (int k = 0; k < n; ++k) h.species.push_back(g.species_names[k]);
+    h.mw.assign(g.mw, g.mw + n);
+    // ---- reaction order: group by kind so a warp group shares one code path
+    auto kind = [&](int r) {
+        int t = g.type[r];
+        int tbl = g.tb_off[r + 1] - g.tb_off[r];
+        if (t == 0) return g.rev[r] ? 1 : 0;
+        if (t == 1) return tbl > 16 ? 3 : 2;
+        return 2 + t;   // 4 Lindemann, 5 Troe
+    };
+    std::vector<int> order(nr);
+    for (int r = 0; r < nr; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return kind(a) < kind(b); });
+    const int ns = ((nr + 32) / 32) * 32;   // at least one padding slot (q == 0)
+    h.nslot = ns;
+    h.slot_rxn.assign(ns, -1);
+    for (int s = 0; s < nr; ++s) h.slot_rxn[s] = order[s];
+
+    std::vector<double> logA(ns, 0), b(ns, 0), EaR(ns, 0), Ac(ns, 0), lnPfac(ns, 0), logA0(ns, 0),
+        b0(ns, 0), EaR0(ns, 0), A0c(ns, 0), ta(ns, 0), tiT3(ns, 0), tiT1(ns, 0), tT2(ns, 0);
+    std::vector<int> flags(ns, 0), rf(3 * ns, n), pf(3 * ns, n), dnu(ns, 0), tboff(ns, 0),
+        tblen(ns, 0), jrow(6 * ns, -1), jnu(6 * ns, 0), catsp(ns, -1);
+    std::vector<int> tbsp;
+    std::vector<double> tbal;
+    const double lnPR = std::log(101325.0 / 8314.4621);
+    for (int s = 0; s < ns; ++s) {
+        int r = h.slot_rxn[s];
+        if (r < 0) continue;
+        int fl = g.type[r] | kFlagActive;
+        if (g.rev[r]) fl |= kFlagRev;
+        if (g.b[r] == 0.0 && g.EaR[r] == 0.0) fl |= kFlagConstK;
+        if (g.b0[r] == 0.0 && g.EaR0[r] == 0.0) fl |= kFlagConstK0;
+        if (g.troeT2[r]) fl |= kFlagT2;
+        flags[s] = fl;
+        logA[s] = g.logA[r]; b[s] = g.b[r]; EaR[s] = g.EaR[r]; Ac[s] = g.A[r];
+        logA0[s] = g.logA0[r]; b0[s] = g.b0[r]; EaR0[s] = g.EaR0[r]; A0c[s] = g.A0[r];
+        if (g.type[r] == 3) {
+            ta[s] = g.troe[4 * r + 0];
+            tiT3[s] = 1.0 / g.troe[4 * r + 1];
+            tiT1[s] = 1.0 / g.troe[4 * r + 2];
+            tT2[s] = g.troe[4 * r + 3];
+        }
+        int nf = 0, npf = 0, d = 0;
+        for (int i = 0; i < P; ++i) {
+            int sp = g.reac_sp[r * P + i];
+            if (sp < 0) break;
+            for (int q = 0; q < g.reac_nu[r * P + i]; ++q) {
+                if (nf >= 3) { *err = "more than 3 reactant molecules"; return HostMech(); }
+                rf[nf * ns + s] = sp; ++nf;
+            }
+            d -= g.reac_nu[r * P + i];
+        }
+        for (int i = 0; i < P; ++i) {
+            int sp = g.prod_sp[r * P + i];
+            if (sp < 0) break;
+            for (int q = 0; q < g.prod_nu[r * P + i]; ++q) {
+                if (npf >= 3) { *err = "more than 3 product molecules"; return HostMech(); }
+                pf[npf * ns + s] = sp; ++npf;
+            }
+            d += g.prod_nu[r * P + i];
+        }
+        dnu[s] = d;
+        lnPfac[s] = d * lnPR;
+        tboff[s] = (int)tbsp.size();
+        // a third-body list of all species but one with alpha = -1 is pyJac's
+        // "single collider" form: keep it as a catalyst species instead
+        const int tl = g.tb_off[r + 1] - g.tb_off[r];
+        bool catalyst = (g.type[r] == 1 && tl == n - 1);
+        if (catalyst) {
+            std::vector<int> seen(n, 0);
+            for (int t = g.tb_off[r]; t < g.tb_off[r + 1]; ++t) {
+                if (g.tb_alpha[t] != -1.0) catalyst = false;
+                seen[g.tb_sp[t]] = 1;
+            }
+            int miss = -1;
+            for (int k = 0; k < n; ++k) if (!seen[k]) miss = k;
+            if (catalyst && miss >= 0) {
+                catsp[s] = miss;
+                flags[s] |= kFlagCatalyst;
+            } else {
+                catalyst = false;
+            }
+        }
+        if (!catalyst) {
+            for (int t = g.tb_off[r]; t < g.tb_off[r + 1]; ++t) {
+                tbsp.push_back(g.tb_sp[t]);
+                tbal.push_back(g.tb_alpha[t]);
+            }
+        }
+        tblen[s] = (int)tbsp.size() - tboff[s];
+        // net stoichiometry rows
+        std::vector<std::pair<int, int>> net;
+        auto add = [&](int sp, int nu) {
+            for (auto& e : net) if (e.first == sp) { e.second += nu; return; }
+            net.push_back({sp, nu});
+        };
+        for (int i = 0; i < P; ++i) { int sp = g.reac_sp[r * P + i]; if (sp < 0) break; add(sp, -g.reac_nu[r * P + i]); }
+        for (int i = 0; i < P; ++i) { int sp = g.prod_sp[r * P + i]; if (sp < 0) break; add(sp, g.prod_nu[r * P + i]); }
+        int nrow = 0;
+        for (auto& e : net) {
+            if (e.second == 0) continue;
+            if (nrow >= 6) { *err = "more than 6 species in one reaction"; return HostMech(); }
+            jrow[nrow * ns + s] = e.first;
+            jnu[nrow * ns + s] = e.second;
+            ++nrow;
+        }
+    }
+    if (tbsp.empty()) { tbsp.push_back(0); tbal.push_back(0.0); }
+    h.ntb = (int)tbsp.size();
+    // ---- species gather list in original reaction order
+    std::vector<int> rxn_slot(nr);
+    for (int s = 0; s < ns; ++s) if (h.slot_rxn[s] >= 0) rxn_slot[h.slot_rxn[s]] = s;
+    std::vector<int> spoff(n + 1, 0), spslot, spnu;
+    for (int k = 0; k < n; ++k) {
+        spoff[k] = (int)spslot.size();
+        for (int r = 0; r < nr; ++r) {
+            int s = rxn_slot[r];
+            for (int e = 0; e < 6; ++e)
+                if (jrow[e * ns + s] == k) { spslot.push_back(s); spnu.push_back(jnu[e * ns + s]); }
+        }
+    }
+    spoff[n] = (int)spslot.size();
+    // balanced gather: cut each species' list into units, deal units to lanes
+    struct Unit { int sp, e0, e1; };
+    std::vector<Unit> units;
+    std::vector<int> unitoff(n + 1, 0);
+    for (int k = 0; k < n; ++k) {
+        unitoff[k] = (int)units.size();
+        for (int e = spoff[k]; e < spoff[k + 1]; e += kGatherUnit)
+            units.push_back({k, e, std::min(e + kGatherUnit, spoff[k + 1])});
+    }
+    unitoff[n] = (int)units.size();
+    std::vector<std::vector<int>> lane_units(32);
+    std::vector<int> load(32, 0);
+    std::vector<int> uorder(units.size());
+    for (size_t u = 0; u < units.size(); ++u) uorder[u] = (int)u;
+    std::stable_sort(uorder.begin(), uorder.end(), [&](int a, int b) {
+        return (units[a].e1 - units[a].e0) > (units[b].e1 - units[b].e0);
+    });
+    for (int u : uorder) {   // longest-first onto the least-loaded lane
+        int best = 0;
+        for (int l = 1; l < 32; ++l) if (load[l] < load[best]) best = l;
+        lane_units[best].push_back(u);
+        load[best] += units[u].e1 - units[u].e0;
+    }
+    int gmax = 1;
+    for (int l = 0; l < 32; ++l) gmax = std::max(gmax, load[l]);
+    const int pad_slot = ns - 1 >= nr ? ns - 1 : -1;   // an inactive slot (q == 0)
+    std::vector<int> gword((size_t)gmax * 32, 0);
+    for (int l = 0; l < 32; ++l) {
+        int e = 0;
+        for (int u : lane_units[l]) {
+            for (int x = units[u].e0; x < units[u].e1; ++x, ++e) {
+                const int last = (x == units[u].e1 - 1) ? 1 : 0;
+                gword[(size_t)e * 32 + l] = spslot[x] | ((spnu[x] + 16) << 11) | (last << 16) | (u << 17);
+            }
+        }
+        for (; e < gmax; ++e) gword[(size_t)e * 32 + l] = (pad_slot >= 0 ? pad_slot : 0) | (16 << 11);
+    }
+    if (pad_slot < 0) { *err = "no padding slot for the gather (reaction count multiple of 32)"; return HostMech(); }
+    if (ns > 2048 || (int)units.size() >= (1 << 15)) { *err = "mechanism too large for the gather encoding"; return HostMech(); }
+    h.gmax = gmax;
+    h.nunit = (int)units.size();
+    if (spslot.empty()) { spslot.push_back(0); spnu.push_back(0); }
+    h.nent = (int)spslot.size();
+    // ---- species arrays
+    std::vector<double> inv_mw(n), tmid(g.tmid, g.tmid + n), nasa(14 * n);
+    for (int k = 0; k < n; ++k) {
+        inv_mw[k] = 1.0 / g.mw[k];
+        for (int i = 0; i < 7; ++i) {
+            nasa[14 * k + i] = g.nasa_lo[7 * k + i];
+            nasa[14 * k + 7 + i] = g.nasa_hi[7 * k + i];
+        }
+    }
+    // ---- serialize
+    auto put = [&](const void* src, size_t bytes) {
+        size_t off = (h.blob.size() + 255) & ~size_t(255);
+        h.blob.resize(off + bytes);
+        std::copy((const unsigned char*)src, (const unsigned char*)src + bytes, h.blob.begin() + off);
+        return off;
+    };
+#define PUTV(v) put((v).data(), (v).size() * sizeof((v)[0]))
+    h.o_mw = put(g.mw, n * sizeof(double));
+    h.o_inv_mw = PUTV(inv_mw);
+    h.o_tmid = PUTV(tmid);
+    h.o_nasa = PUTV(nasa);
+    h.o_logA = PUTV(logA); h.o_b = PUTV(b); h.o_EaR = PUTV(EaR); h.o_Aconst = PUTV(Ac);
+    h.o_lnPfac = PUTV(lnPfac); h.o_logA0 = PUTV(logA0); h.o_b0 = PUTV(b0); h.o_EaR0 = PUTV(EaR0);
+    h.o_A0const = PUTV(A0c); h.o_troe_a = PUTV(ta); h.o_troe_iT3 = PUTV(tiT3);
+    h.o_troe_iT1 = PUTV(tiT1); h.o_troe_T2 = PUTV(tT2); h.o_flags = PUTV(flags);
+    h.o_rf = PUTV(rf); h.o_pf = PUTV(pf); h.o_dnu = PUTV(dnu); h.o_tb_off = PUTV(tboff);
+    h.o_tb_len = PUTV(tblen); h.o_tb_sp = PUTV(tbsp); h.o_tb_alpha = PUTV(tbal);
+    h.o_jrow = PUTV(jrow); h.o_jnu = PUTV(jnu); h.o_sp_off = PUTV(spoff);
+    h.o_sp_slot = PUTV(spslot); h.o_sp_nu = PUTV(spnu);
+    h.o_cat_sp = PUTV(catsp); h.o_gword = PUTV(gword); h.o_unit_off = PUTV(unitoff);
+#undef PUTV
+    h.blob.resize((h.blob.size() + 255) & ~size_t(255));
+    return h;
+}
+
+}  // namespace b200

@@ -390,9 +390,16 @@ class Mechanism:
             f.write("\n".join(lines) + "\n")
         # sidecar with what host code needs without parsing C
         import json
+        rx = []
+        for r in self.reactions:
+            net = r.net_stoich(n)
+            rx.append({"type": r.rtype, "rev": int(r.reversible),
+                       "nf": sum(v for _, v in r.reac), "np": sum(v for _, v in r.prod),
+                       "tb": len(r.tb), "nrow": len(net),
+                       "constk": int(r.b == 0.0 and r.EaR == 0.0), "T2": int(r.troe_has_T2)})
         side = {"name": self.name, "nsp": n, "nrxn": nr,
                 "species": [s.name for s in self.species],
-                "mw": [s.mw for s in self.species], "counts": self.counts()}
+                "mw": [s.mw for s in self.species], "counts": self.counts(), "reactions": rx}
         with open(os.path.splitext(path)[0] + ".json", "w") as f:
             json.dump(side, f, indent=1)
 

@@ -1,0 +1,160 @@
+/* b200ode -- C ABI of the B200 batched stiff-chemistry BDF integrator.
+ *
+ * This is the boundary the host-side Integrator subclass (B200BDFIntegrator,
+ * include/b200ode_integrator.hpp) calls.  It replaces, for one batch of
+ * cells, what the reference's GPU path does inside
+ *   CVodeIntegratorGPU::integrate / integrateBatch
+ *     src/Integrators/CVodeIntegratorGPU.cpp:30-126
+ *   (calc_gpu_points, init_memory_gpu, N_VNew_Cuda, CVodeCreate(CV_BDF),
+ *    SUNMatrix_MagmaDenseBlock, SUNLinSol_MagmaDense, CVode(..., CV_NORMAL),
+ *    saveGPUArrayResults; src/Integrators/Drivers/CVodeGPUDriver.cu:28-398)
+ * and what the serial oracle path does per cell in
+ *   CVodeIntegrator::integrateSystem  src/Integrators/CVodeIntegrator.cpp:98-155.
+ *
+ * Semantics are those of the serial CVODE path: every cell runs its own
+ * variable-order BDF (own step size, order and error test), to tout = t1 in
+ * CV_NORMAL mode, with scalar reltol/abstol (CVodeSStolerances) and
+ * max_steps (CVodeSetMaxNumSteps, 10000 in the reference).  The state of a cell
+ * is [T, Y_0 .. Y_{nsp-2}]; the last species is returned as 1 - sum(Y_k)
+ * (CVodeIntegrator.cpp:79-96).
+ *
+ * Data layout: structure of arrays, cell index innermost.  Y is nsp x n_cells
+ * (Y[k * n_cells + c]), T and P are n_cells long.  Plain pointers, no C++ types,
+ * no exceptions cross the ABI.  The caller owns every host buffer; the library
+ * owns its device buffers.  A handle is used by one host thread at a time.
+ */
+#ifndef B200ODE_H
+#define B200ODE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct b200ode_handle b200ode_handle;
+
+typedef enum {
+    B200ODE_OK = 0,
+    B200ODE_ERR_INVALID = 1,     /* bad argument (null pointer, size, tolerance ...) */
+    B200ODE_ERR_MECHANISM = 2,   /* unknown mechanism or species-count mismatch */
+    B200ODE_ERR_CUDA = 3,        /* CUDA runtime error (message in b200ode_last_error) */
+    B200ODE_ERR_ALLOC = 4,       /* device or pinned allocation failed */
+    B200ODE_ERR_NO_DEVICE = 5,   /* no usable CUDA device */
+    B200ODE_ERR_BUSY = 6,        /* serving queue full */
+    B200ODE_ERR_NOT_READY = 7    /* serving request still in flight */
+} b200ode_status;
+
+/* Per-cell integration status: CVODE return codes (CVode() return values). */
+enum {
+    B200ODE_CELL_SUCCESS = 0,
+    B200ODE_CELL_TOO_MUCH_WORK = -1,   /* CV_TOO_MUCH_WORK: max_steps reached */
+    B200ODE_CELL_TOO_MUCH_ACC = -2,    /* CV_TOO_MUCH_ACC */
+    B200ODE_CELL_ERR_FAILURE = -3,     /* CV_ERR_FAILURE: 7 error-test failures in one step */
+    B200ODE_CELL_CONV_FAILURE = -4,    /* CV_CONV_FAILURE: 10 convergence failures in one step */
+    B200ODE_CELL_TOO_CLOSE = -27       /* CV_TOO_CLOSE: t1 too close to t0 */
+};
+
+typedef enum { B200ODE_FP64 = 0, B200ODE_MIXED = 1 } b200ode_precision;
+
+typedef struct {
+    double reltol;            /* CVodeSStolerances reltol (reference: 1e-6) */
+    double abstol;            /* CVodeSStolerances abstol (reference: 1e-10) */
+    int32_t max_steps;        /* CVodeSetMaxNumSteps (reference: 10000) */
+    int32_t max_order;        /* BDF max order, 1..5 (CVODE default 5) */
+    int32_t precision;        /* B200ODE_FP64 or B200ODE_MIXED (FP32 Jacobian/LU/solve) */
+    int32_t refine;           /* mixed only: 1 = one FP64-residual refinement sweep per solve */
+    int32_t persistent;       /* 1 = persistent kernel + device work queue; 0 = one launch per BDF step */
+    int32_t warps_per_block;  /* 0 = from the autotuner / occupancy */
+    int32_t blocks_per_sm;    /* 0 = from occupancy */
+    int32_t queue_chunk;      /* cells a warp takes from the work queue at once (0 = 1) */
+    int32_t use_graph;        /* one-launch-per-step form: capture the step launches in a CUDA graph */
+    int32_t device;           /* CUDA device ordinal (-1 = current) */
+    int32_t profile_phases;   /* 1 = accumulate per-phase device cycles into b200ode_stats */
+} b200ode_options;
+
+/* Optional per-cell counters (CVodeGetNum* equivalents) and call totals.  Any
+ * per-cell pointer may be NULL.  Totals and timings are always filled. */
+typedef struct {
+    int32_t* nst;        /* steps */
+    int32_t* nfe;        /* RHS evaluations */
+    int32_t* nje;        /* Jacobian evaluations */
+    int32_t* nsetups;    /* Newton-matrix setups (LU factorizations) */
+    int32_t* nni;        /* Newton iterations (linear solves) */
+    int32_t* ncfn;       /* nonlinear convergence failures */
+    int32_t* netf;       /* error-test failures */
+    int64_t total_nst, total_nfe, total_nje, total_nsetups, total_nni, total_ncfn, total_netf;
+    int64_t n_failed;        /* cells whose status != B200ODE_CELL_SUCCESS */
+    double h2d_ms, kernel_ms, d2h_ms;   /* device-timed phases of the last call */
+    int32_t gpu_launches;    /* kernels this library launched in the last call */
+    int64_t phase_cycles[5]; /* profile_phases: SM cycles summed over warps in RHS, Jacobian,
+                                LU, triangular solves, and the whole kernel (persistent form) */
+} b200ode_stats;
+
+/* Fill *opts with the reference's settings (1e-6 / 1e-10 / 10000 / order 5),
+ * mixed precision, persistent kernel. */
+void b200ode_default_options(b200ode_options* opts);
+
+/* Create a handle for a mechanism ("gri30", "gri30.yaml", "h2o2", "h2o2.yaml").
+ * Replaces the per-batch set-up of CVodeIntegratorGPU::integrateBatch
+ * (CVodeIntegratorGPU.cpp:44-100) and CVodeIntegrator::init's NSP check
+ * (CVodeIntegrator.cpp:34-50).  opts may be NULL (defaults). */
+b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts,
+                              b200ode_handle** out);
+void b200ode_destroy(b200ode_handle* h);
+
+/* Number of species of the handle's mechanism (the reference's NSP). */
+int32_t b200ode_num_species(const b200ode_handle* h);
+
+/* Integrate n_cells cells from t0 to t1 (host buffers, synchronous).
+ * P: per-cell pressure [Pa] (n_cells) or NULL to use P_scalar (the reference's
+ * IntegratorConfig::pressure, Integrator.hpp:13-19).  T (n_cells) and Y
+ * (nsp x n_cells, SoA) are read and overwritten.  cell_status (n_cells) may be
+ * NULL.  stats may be NULL.  Cells that fail keep the last accepted state, as
+ * CVode returns it. */
+b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n_cells, const double* P,
+                                 double P_scalar, double* T, double* Y, double t0, double t1,
+                                 int32_t* cell_status, b200ode_stats* stats);
+
+/* Same on device-resident buffers (no host copies; stream is a cudaStream_t or
+ * NULL for the legacy default stream).  Asynchronous with respect to the host
+ * unless stats is non-NULL (then it synchronizes the stream to fill totals;
+ * per-cell counter pointers must be device pointers). */
+b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, const double* d_P,
+                                        double P_scalar, double* d_T, double* d_Y, double t0,
+                                        double t1, int32_t* d_cell_status, b200ode_stats* stats,
+                                        void* stream);
+
+/* Chemistry source terms alone, one GPU warp per cell (host buffers).
+ * Counterparts of the reference's batched pyJac kernels dydt_cvode_GPU /
+ * kernel_dydt (src/Integrators/Drivers/CVodeGPUDriver.cu:28-65, 299-313) and of
+ * pyJac's dydt (src/Mechanism/CPU/dydt.c:7): T, Y as in b200ode_integrate;
+ * dTdt (n_cells) and dYdt ((nsp-1) x n_cells, SoA) receive d/dt of the state
+ * [T, Y_0 .. Y_{nsp-2}].  Arithmetic in FP64. */
+b200ode_status b200ode_eval_rhs(b200ode_handle* h, int64_t n_cells, const double* P, double P_scalar,
+                                const double* T, const double* Y, double* dTdt, double* dYdt);
+
+/* Analytic Jacobian, one GPU warp per cell.  Counterpart of
+ * jacobian_cvode_GPU / kernel_eval_jacob (CVodeGPUDriver.cu:67-106, 338-354)
+ * and pyJac's eval_jacob (src/Mechanism/CPU/jacob.c:3): jac receives, per cell,
+ * nsp x nsp column-major d f_i / d y_j with y = [T, Y_0 .. Y_{nsp-2}]
+ * (jac[c*nsp*nsp + i + nsp*j]).  Computed in the handle's Newton-matrix
+ * precision (FP32 for B200ODE_MIXED, FP64 otherwise). */
+b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n_cells, const double* P,
+                                     double P_scalar, const double* T, const double* Y, double* jac);
+
+/* Diagnostic: measured FP64 FMA throughput of a device (GFLOP/s), the
+ * denominator of the FP64-pipe roofline this library reports.  No reference
+ * counterpart (a measurement helper). */
+b200ode_status b200ode_fp64_peak(int32_t device, double* gflops);
+
+/* Message of the last error on this thread ("" if none). */
+const char* b200ode_last_error(void);
+
+/* Library version string. */
+const char* b200ode_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200ODE_H */

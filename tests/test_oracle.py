@@ -1,0 +1,117 @@
+"""CPU oracle checks: pinned against the reference's own pyJac outputs (golden
+vectors generated from the compiled reference C by tests/golden/make_golden.py)
+and against scipy's VODE/Radau."""
+import numpy as np
+import pytest
+
+from hpc_ode_b200 import workloads as W
+
+
+def test_mechanism_tables_match_pyjac_structure():
+    g = W.mech_info("gri30")
+    c = g["counts"]
+    # src/Mechanism/CPU/mechanism.h:63-71: NSP 53, FWD_RATES 325, REV_RATES 309, PRES_MOD_RATES 50
+    assert (c["species"], c["reactions"], c["reversible"], c["pres_mod"]) == (53, 325, 309, 50)
+    assert c["troe"] == 26 and c["lindemann"] == 3 and c["three-body"] == 21
+    assert g["species"][-1] == "CH3CHO"          # mechanism.h:5 last_spec 52
+    h = W.mech_info("h2o2")
+    assert h["nsp"] == 10 and h["counts"]["reactions"] == 29 and h["species"][-1] == "N2"
+
+
+def test_rhs_matches_reference_pyjac(oracle, golden_chem):
+    y, P, ref = golden_chem["y"], golden_chem["P"], golden_chem["dydt"]
+    worst = 0.0
+    for i in range(len(P)):
+        got = oracle.dydt("gri30", P[i], y[i])
+        scale = oracle.dydt_scale("gri30", P[i], y[i])
+        err = np.abs(got - ref[i]) / (np.abs(ref[i]) + scale + 1e-300)
+        worst = max(worst, err.max())
+    # cancellation-aware relative tolerance (scale = |fwd| + |rev| contributions)
+    assert worst <= 1e-12, worst
+
+
+def test_jacobian_matches_reference_pyjac(oracle, golden_chem):
+    y, P, ref = golden_chem["y"], golden_chem["P"], golden_chem["jac"]
+    for i in range(int(golden_chem["jac_count"])):
+        J = oracle.jacob("gri30", P[i], y[i])
+        Jr = ref[i]
+        mask = np.abs(Jr) > 1e-8 * np.abs(Jr).max()
+        mask[0, 0] = False   # pyJac's dTdot/dT is not the derivative of its dydt (see next test)
+        rel = np.abs(J - Jr)[mask] / np.abs(Jr)[mask]
+        assert rel.max() <= 1e-10, (i, rel.max())
+
+
+def test_jacobian_TT_is_derivative_of_reference_rhs(oracle, golden_chem):
+    """J[0,0] against central differences of the reference pyJac dydt values
+    (the oracle's dydt equals pyJac's to 1e-12)."""
+    y, P = golden_chem["y"], golden_chem["P"]
+    for i in range(8):
+        J = oracle.jacob("gri30", P[i], y[i])
+        h = 1e-3
+        yp, ym = y[i].copy(), y[i].copy()
+        yp[0] += h
+        ym[0] -= h
+        fd = (oracle.dydt("gri30", P[i], yp)[0] - oracle.dydt("gri30", P[i], ym)[0]) / (2 * h)
+        assert abs(J[0, 0] - fd) <= 1e-5 * max(abs(fd), 1.0), (i, J[0, 0], fd)
+
+
+@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k")])
+def test_jacobian_finite_difference(oracle, mech, wl):
+    b = W.make(wl, 4, seed=7)
+    ys = b.state_rows()
+    for c in range(4):
+        y = ys[c]
+        J = oracle.jacob(mech, b.P[c], y)
+        n = y.size
+        Jfd = np.zeros((n, n))
+        for j in range(n):
+            h = 1e-4 if j == 0 else 1e-7 * max(abs(y[j]), 1e-8)
+            yp, ym = y.copy(), y.copy()
+            yp[j] += h
+            ym[j] -= h
+            Jfd[:, j] = (oracle.dydt(mech, b.P[c], yp) - oracle.dydt(mech, b.P[c], ym)) / (2 * h)
+        big = np.abs(Jfd) > 1e-4 * np.abs(Jfd).max()
+        rel = np.abs(J - Jfd)[big] / np.abs(Jfd)[big]
+        assert np.quantile(rel, 0.99) < 1e-3 and rel.max() < 1e-2, (c, rel.max())
+
+
+def test_bdf_matches_scipy_radau(oracle):
+    from scipy.integrate import solve_ivp
+    for wl, n in (("h2_1024", 3), ("gri_32k", 3)):
+        b = W.make(wl, n)
+        ys = b.state_rows()
+        yt, st = oracle.bdf(b.mech, ys, b.P, b.dt, rtol=1e-10, atol=1e-14)
+        assert (st["status"] == 0).all()
+        for c in range(n):
+            f = lambda t, y: oracle.dydt(b.mech, b.P[c], y)  # noqa: E731
+            J = lambda t, y: oracle.jacob(b.mech, b.P[c], y)  # noqa: E731
+            r = solve_ivp(f, (0, b.dt), ys[c], method="Radau", jac=J, rtol=1e-11, atol=1e-15)
+            assert abs(yt[c, 0] - r.y[0, -1]) / r.y[0, -1] < 1e-8
+
+
+def test_quiescent_e2e_fixture(oracle, golden_e2e):
+    """The reference's 99-cell 300 K E2E case comes back as the reference's serial
+    CVODE output (E2Etests/100/results_serial100.csv)."""
+    g = golden_e2e
+    y = np.concatenate([g["T_in"][:, None], g["Y_in"][:, :-1]], axis=1)
+    yo, st = oracle.bdf("gri30", y, float(g["P"]), float(g["dt"]), threads=4)
+    assert (st["status"] == 0).all()
+    assert np.abs(yo[:, 0] - g["T_out"]).max() <= 1e-9 * 300.0
+    assert np.abs(yo[:, 1:] - g["Y_out"][:, :-1]).max() <= 1e-20
+
+
+def test_openmp_batch_equals_serial(oracle):
+    """As the reference's testSerialvsOMP (tests/Integrators/testCVodeIntegrator.cpp:92-134):
+    the threaded batch equals the serial batch bit for bit."""
+    b = W.make("h2_1024", 16)
+    y1, s1 = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, threads=1)
+    y4, s4 = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, threads=4)
+    assert np.array_equal(y1, y4) and np.array_equal(s1, s4)
+
+
+def test_max_steps_cap_and_too_close(oracle):
+    b = W.make("gri_1m", 2)
+    y, st = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, max_steps=5)
+    assert (st["status"] == -1).all() and (st["nst"] == 5).all()
+    y, st = oracle.bdf(b.mech, b.state_rows(), b.P, 0.0)
+    assert (st["status"] == -27).all()
