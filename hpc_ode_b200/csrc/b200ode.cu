@@ -132,24 +132,19 @@ __device__ __forceinline__ void store_cell(const KParams& p, long long cell, int
 // allow (1 -> up to 255 registers, 3 -> at most 168); chosen by the autotuner.
 template <class MT, class LinT, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KParams p) {
-    using B = WarpBdf<MT, LinT>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using R = StepRecord<MT, LinT>;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    auto* w = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
+    const unsigned off = smem_off(w);
+    BdfState& S = w->st;
     const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     const bool step_form = p.records != nullptr;
     auto* wglob = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal);
-    B bdf(sm, wglob + gw, lane);
-    bdf.rtol = p.rtol;
-    bdf.atol = p.atol;
-    bdf.max_steps = p.max_steps;
-    bdf.qmax = p.max_order;
-    bdf.refine = p.refine;
-    bdf.profiling = p.prof != nullptr;
-    if (lane < 8) sm->prof[lane] = 0;
+    const int profiling = (p.prof != nullptr && !step_form) ? 1 : 0;
+    if (lane < 8) S.prof[lane] = 0;
     __syncwarp();
-    const long long t_start = bdf.profiling ? clock64() : 0;
+    const long long t_start = profiling ? clock64() : 0;
     unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long cell = gw;
 #pragma unroll 1
@@ -163,49 +158,48 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
             if (c >= (unsigned long long)p.ncells) break;
             cell = (long long)c;
         }
-        unsigned char* rec = step_form ? p.records + cell * (long long)B::kRecordBytes : nullptr;
-        int phase = step_form ? reinterpret_cast<const typename B::Scalars*>(rec)->phase : 0;
+        WarpGlobal<MT, LinT>* wg = wglob + (step_form ? cell : gw);
+        unsigned char* rec = step_form ? p.records + cell * (long long)R::kBytes : nullptr;
+        const int phase = step_form ? *reinterpret_cast<const int*>(rec + R::kPhaseOff) : 0;
         if (phase == 2) continue;
+        if (phase != 0) bdf_load<MT, LinT>(off, rec, lane);
+        S.rtol = p.rtol;
+        S.atol = p.atol;
+        S.max_steps = p.max_steps;
+        S.qmax = p.max_order;
+        S.refine = p.refine;
+        S.profiling = profiling;
+        S.lu_dirty = 0;
         int status = 0;
         bool done = false;
-        bdf.lu_dirty = 0;
         if (phase == 0) {
-            double y0[MT::NS];
-            load_cell<MT>(p, cell, lane, y0);
-            bdf.P = p.P ? p.P[cell] : p.P_scalar;
-            status = bdf.begin(y0, p.t0, p.t1);
+            Vec<MT::NS> y0;
+            load_cell<MT>(p, cell, lane, y0.v);
+            S.P = p.P ? p.P[cell] : p.P_scalar;
+            status = bdf_begin<MT, LinT>(off, y0, p.t0, p.t1, lane);
             done = (status != 0);
-        } else {
-            bdf.load(rec, status, phase);
         }
-        if (!done) status = bdf.advance(p.t1, p.steps, done);
+        if (!done) status = bdf_advance<MT, LinT>(off, wg, p.t1, p.steps, done, lane);
         if (done) {
-            double yo[MT::NS];
-            bdf.finish(status, p.t1, yo);
-            store_cell<MT>(p, cell, lane, yo);
-            const CellCounters& c = bdf.cnt;
+            const Vec<MT::NS> yo = bdf_finish<MT, LinT>(off, status, p.t1, lane);
+            store_cell<MT>(p, cell, lane, yo.v);
             if (lane == 0) {
                 if (p.status) p.status[cell] = status;
-                if (p.cnt[0]) p.cnt[0][cell] = c.nst;
-                if (p.cnt[1]) p.cnt[1][cell] = c.nfe;
-                if (p.cnt[2]) p.cnt[2][cell] = c.nje;
-                if (p.cnt[3]) p.cnt[3][cell] = c.nsetups;
-                if (p.cnt[4]) p.cnt[4][cell] = c.nni;
-                if (p.cnt[5]) p.cnt[5][cell] = c.ncfn;
-                if (p.cnt[6]) p.cnt[6][cell] = c.netf;
+                for (int i = 0; i < 7; ++i)
+                    if (p.cnt[i]) p.cnt[i][cell] = S.cnt[i];
                 if (step_form) atomicAdd(p.done_count, 1ULL);
             }
-            tot[0] += c.nst; tot[1] += c.nfe; tot[2] += c.nje; tot[3] += c.nsetups;
-            tot[4] += c.nni; tot[5] += c.ncfn; tot[6] += c.netf; tot[7] += (status != 0);
+            for (int i = 0; i < 7; ++i) tot[i] += (unsigned long long)S.cnt[i];
+            tot[7] += (status != 0);
         }
-        if (step_form) bdf.save(rec, status, done ? 2 : 1, bdf.lu_dirty != 0);
+        if (step_form) bdf_save<MT, LinT>(off, rec, done ? 2 : 1, lane);
     }
     if (lane == 0)
         for (int i = 0; i < 8; ++i)
             if (tot[i]) atomicAdd(p.totals + i, tot[i]);
-    if (bdf.profiling && lane == 0) {
-        sm->prof[PH_TOTAL] = clock64() - t_start;
-        for (int i = 0; i < 5; ++i) atomicAdd(p.prof + i, (unsigned long long)sm->prof[i]);
+    if (profiling && lane == 0) {
+        S.prof[PH_TOTAL] = clock64() - t_start;
+        for (int i = 0; i < 5; ++i) atomicAdd(p.prof + i, (unsigned long long)S.prof[i]);
     }
 }
 
@@ -215,15 +209,14 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
 // outputs in the reference's layout.
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParams p, double* dTdt, double* dYdt) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (cell >= p.ncells) return;
-    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     Vec<MT::NS> y;
     load_cell<MT>(p, cell, lane, y.v);
     const double P = p.P ? p.P[cell] : p.P_scalar;
-    const Vec<MT::NS> f = warp_rhs<MT>(P, y, &sm->chem, lane);
+    const Vec<MT::NS> f = warp_rhs<MT>(P, y, smem_off(&sm->chem), lane);
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
         const int i = lane + 32 * s;
@@ -235,16 +228,15 @@ __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParam
 // jac: per cell N*N column-major, reference order [T, Y_0 .. Y_{N-2}].
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParams p, double* jac) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (cell >= p.ncells) return;
-    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(smem_raw) + wib;
+    auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     auto* wg = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal) + cell;
     Vec<MT::NS> y;
     load_cell<MT>(p, cell, lane, y.v);
     const double P = p.P ? p.P[cell] : p.P_scalar;
-    warp_jac<MT, LinT>(P, y, sm->A, &sm->chem, &wg->js, lane);
+    warp_jac<MT, LinT>(P, y, smem_off(sm->A), smem_off(&sm->chem), &wg->js, lane);
     constexpr int N = MT::N;
     double* out = jac + cell * (long long)(N * N);
     for (int i = 0; i < N; ++i)
@@ -313,7 +305,7 @@ b200ode_status ensure_wg(b200ode_handle* h, size_t bytes) {
 
 template <class MT, class LinT>
 b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
-    using B = WarpBdf<MT, LinT>;
+    using R = StepRecord<MT, LinT>;
     const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
     auto kern = k_bdf<MT, LinT, 1>;
@@ -345,7 +337,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     // one launch per BDF step: per-cell scratch and state records in HBM
     b200ode_status rc = ensure_wg(h, n * sizeof(WarpGlobal<MT, LinT>));
     if (rc != B200ODE_OK) return rc;
-    const size_t rb = n * B::kRecordBytes;
+    const size_t rb = n * R::kBytes;
     if (rb > h->rec_bytes) {
         if (h->d_rec) cudaFree(h->d_rec);
         h->d_rec = nullptr;

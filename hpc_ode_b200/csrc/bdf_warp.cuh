@@ -19,12 +19,15 @@
 // interpolation at tout.  The CPU oracle (oracle/bdf_oracle.c) is the same
 // algorithm in scalar C; the GPU kernel is checked against it.
 //
-// Storage: the Nordsieck history and the method arrays (l, tq, tau) live in
-// the warp's shared memory (compact rolled loops, few registers); the work
-// vectors (ewt, acor, y, ftemp, ...) are lane registers (element i = lane +
-// 32 s, internal order Y_0..Y_{N-2}, T).  Scalars are computed identically by
-// all 32 lanes from identical warp-reduced values, so control flow is uniform
-// across the warp; shared arrays are written by every lane with the same value.
+// Layout for a small instruction footprint: the method state (scalars, l, tq,
+// tau, counters) and the Nordsieck history live in the warp's shared memory;
+// every lane computes the same scalar values and writes them (identical
+// values, so the shared words are consistent).  Work vectors (ewt, acor, y,
+// ftemp, delta) are lane registers (element i = lane + 32 s; internal order
+// Y_0..Y_{N-2}, T).  Only the Newton loop is inlined; step-size/order
+// selection, coefficient updates, the linear-solver setup, the initial step and
+// the HBM record I/O are single out-of-line copies addressed by a shared-memory
+// offset, so the kernel's hot code stays inside the instruction cache.
 // Every loop is bounded (max_steps, 10 convergence failures, 7 error-test
 // failures, 3 Newton iterations), so a cell cannot spin.
 #pragma once
@@ -52,17 +55,29 @@ enum { CV_SUCCESS = 0, CV_TOO_MUCH_WORK = -1, CV_TOO_MUCH_ACC = -2, CV_ERR_FAILU
 
 // Phases of the per-phase cycle profile.
 enum { PH_RHS = 0, PH_JAC = 1, PH_LU = 2, PH_SOLVE = 3, PH_TOTAL = 4 };
+enum { C_NST = 0, C_NFE, C_NJE, C_NSETUPS, C_NNI, C_NCFN, C_NETF };
+
+// Method state of one cell (CVODE's cv_mem scalars), in shared memory.
+struct BdfState {
+    double l[8], tq[8], tau[8];
+    double tn, h, hprime, hscale, eta, etamax, hu, saved_tq5;
+    double gamma, gammap, gamrat, rl1, crate, acnrm, etaq, etaqm1, etaqp1;
+    double P, rtol, atol;
+    int q, qprime, qwait, L, indx_acor, jcur, convfail;
+    int nst, nstlp, nstlj, nstloc, max_steps, qmax, refine, lu_dirty, profiling;
+    int cnt[7];
+    long long prof[8];   // per-phase clock64 totals when profiling
+};
 
 // Per-warp shared memory.
 template <class MT, class LinT>
 struct WarpSmem {
     ChemSmem<MT> chem;
     double zn[cv::QMAX + 1][32 * MT::NS];   // Nordsieck history zn[j][i]
-    double l[8], tq[8], tau[8];             // method coefficients (l[0..q], tq[1..5], tau[1..q+1])
+    BdfState st;
     LinT A[MT::N * MT::LDA];                // Jacobian, then the LU factors of M = I - gamma J
     LinT dinv[MT::N];
     int perm[MT::N];
-    long long prof[8];                      // per-phase clock64 totals when profiling
 };
 
 // Per-warp global scratch: saved Jacobian (CVODE keeps it to form new M
@@ -73,132 +88,100 @@ struct WarpGlobal {
     JacScratch<MT> js;
 };
 
-struct CellCounters {
-    int nst, nfe, nje, nsetups, nni, ncfn, netf;
-};
+template <class MT, class LinT>
+__device__ __forceinline__ WarpSmem<MT, LinT>* wsm(unsigned off) {
+    return smem_at<WarpSmem<MT, LinT>>(off);
+}
+
+template <int NS>
+__device__ __forceinline__ bool valid_el(int lane, int s, int N) { return lane + 32 * s < N; }
+
+template <int NS>
+__device__ __forceinline__ double wrms_v(const double (&x)[NS], const double (&w)[NS], int N) {
+    double acc = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) { const double t = x[s] * w[s]; acc += t * t; }
+    return sqrt(warp_sum(acc) / N);
+}
 
 template <class MT, class LinT>
-struct WarpBdf {
-    static constexpr int N = MT::N, NS = MT::NS;
-    // problem
-    double P, rtol, atol;
-    int max_steps, qmax, refine, lane;
-    WarpSmem<MT, LinT>* sm;
-    WarpGlobal<MT, LinT>* wg;
-    // work vectors (lane elements)
-    double ewt[NS], acor[NS], tempv[NS], ftemp[NS], y[NS], delta[NS];
-    // method scalars (identical on all lanes)
-    double tn, h, hprime, hscale, eta, etamax, hu, saved_tq5;
-    double gamma, gammap, gamrat, rl1, crate, acnrm, etaq, etaqm1, etaqp1;
-    int q, qprime, qwait, L, indx_acor, jcur, convfail;
-    int nst, nstlp, nstlj, nstloc;
-    int lu_dirty;   // an LU was computed since the last save (step form)
-    int profiling;  // accumulate per-phase clock64 into sm->prof
-    CellCounters cnt;
+__device__ __forceinline__ double wrms_zn(const WarpSmem<MT, LinT>* w, int j, const double (&ewt)[MT::NS], int lane) {
+    double acc = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) { const double t = w->zn[j][lane + 32 * s] * ewt[s]; acc += t * t; }
+    return sqrt(warp_sum(acc) / MT::N);
+}
 
-    __device__ __forceinline__ WarpBdf(WarpSmem<MT, LinT>* sm_, WarpGlobal<MT, LinT>* wg_, int lane_)
-        : lane(lane_), sm(sm_), wg(wg_) {}
+__device__ __forceinline__ long long ph_tick(const BdfState& S) { return S.profiling ? clock64() : 0; }
+__device__ __forceinline__ void ph_tock(BdfState& S, int ph, long long t0, int lane) {
+    if (S.profiling && lane == 0) S.prof[ph] += clock64() - t0;
+}
 
-    __device__ __forceinline__ bool valid(int s) const { return lane + 32 * s < N; }
-    __device__ __forceinline__ double* zn(int j) const { return sm->zn[j] + lane; }
+// f(y) for the warp's cell (counted as one RHS evaluation).
+template <class MT, class LinT>
+__device__ __forceinline__ void bdf_rhs(unsigned off, const double (&y)[MT::NS], double (&out)[MT::NS], int lane) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    const long long t0 = ph_tick(w->st);
+    Vec<MT::NS> a;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) a.v[s] = y[s];
+    const Vec<MT::NS> r = warp_rhs<MT>(w->st.P, a, smem_off(&w->chem), lane);
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) out[s] = r.v[s];
+    w->st.cnt[C_NFE]++;
+    ph_tock(w->st, PH_RHS, t0, lane);
+}
 
-    __device__ __forceinline__ double wrms(const double (&x)[NS]) const {
-        double acc = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) { const double t = x[s] * ewt[s]; acc += t * t; }
-        return sqrt(warp_sum(acc) / N);
-    }
-    __device__ __forceinline__ double wrms_zn(int j) const {
-        const double* z = zn(j);
-        double acc = 0.0;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) { const double t = z[32 * s] * ewt[s]; acc += t * t; }
-        return sqrt(warp_sum(acc) / N);
-    }
-    __device__ __forceinline__ void set_ewt_zn0() {
-        const double* z = zn(0);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) ewt[s] = valid(s) ? 1.0 / (rtol * fabs(z[32 * s]) + atol) : 0.0;
-    }
-    __device__ __forceinline__ long long tick() const { return profiling ? clock64() : 0; }
-    __device__ __forceinline__ void tock(int ph, long long t0) {
-        if (profiling && lane == 0) sm->prof[ph] += clock64() - t0;
-    }
-    __device__ __forceinline__ void rhs(const double (&yy)[NS], double (&out)[NS]) {
-        const long long t0 = tick();
-        Vec<NS> a;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) a.v[s] = yy[s];
-        const Vec<NS> r = warp_rhs<MT>(P, a, &sm->chem, lane);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) out[s] = r.v[s];
-        cnt.nfe++;
-        tock(PH_RHS, t0);
-    }
-    __device__ __forceinline__ void rhs_zn0(double (&out)[NS]) {
-        double a[NS];
-        const double* z = zn(0);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) a[s] = z[32 * s];
-        rhs(a, out);
-    }
-    __device__ __forceinline__ void lu_solve(double (&b)[NS]) {
-        const long long t0 = tick();
-        Vec<NS> a;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) a.v[s] = b[s];
-        const Vec<NS> r = warp_lu_solve<MT, LinT>(sm->A, sm->perm, sm->dinv, a, lane);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) b[s] = r.v[s];
-        tock(PH_SOLVE, t0);
-    }
-
-    // ----------------------------------------------------------- Nordsieck
-    __device__ __forceinline__ void rescale() {
-        double factor = eta;
+// ---------------------------------------------------------------- Nordsieck
+template <class MT, class LinT>
+__device__ __forceinline__ void bdf_rescale(unsigned off, int lane) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    const double eta = S.eta;
+    double factor = eta;
+    const int q = S.q;
 #pragma unroll 1
-        for (int j = 1; j <= q; ++j) {
-            double* z = zn(j);
+    for (int j = 1; j <= q; ++j) {
 #pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] *= factor;
-            factor *= eta;
-        }
-        h = hscale * eta;
-        hscale = h;
+        for (int s = 0; s < MT::NS; ++s) w->zn[j][lane + 32 * s] *= factor;
+        factor *= eta;
     }
-    __device__ __forceinline__ void predict() {
-        tn += h;
+    S.h = S.hscale * eta;
+    S.hscale = S.h;
+}
+
+// zn <- Pascal-triangle prediction (sign = +1) or its inverse (sign = -1).
+template <class MT, class LinT>
+__device__ __forceinline__ void bdf_pascal(unsigned off, int lane, bool forward) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    const int q = w->st.q;
 #pragma unroll 1
-        for (int k = 1; k <= q; ++k)
+    for (int k = 1; k <= q; ++k)
 #pragma unroll 1
-            for (int j = q; j >= k; --j) {
-                double* a = zn(j - 1);
-                const double* b = zn(j);
+        for (int j = q; j >= k; --j)
 #pragma unroll
-                for (int s = 0; s < NS; ++s) a[32 * s] += b[32 * s];
+            for (int s = 0; s < MT::NS; ++s) {
+                const int i = lane + 32 * s;
+                w->zn[j - 1][i] = forward ? w->zn[j - 1][i] + w->zn[j][i] : w->zn[j - 1][i] - w->zn[j][i];
             }
-    }
-    __device__ __forceinline__ void restore(double saved_t) {
-        tn = saved_t;
-#pragma unroll 1
-        for (int k = 1; k <= q; ++k)
-#pragma unroll 1
-            for (int j = q; j >= k; --j) {
-                double* a = zn(j - 1);
-                const double* b = zn(j);
-#pragma unroll
-                for (int s = 0; s < NS; ++s) a[32 * s] -= b[32 * s];
-            }
-    }
-    __device__ __forceinline__ void increase_bdf() {
-        double* l = sm->l;
-        const double* tau = sm->tau;
-        for (int j = 0; j <= cv::QMAX; ++j) l[j] = 0.0;
-        l[2] = 1.0;
-        double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = hscale;
+}
+
+// Order change by +-1 of the Nordsieck array (CVODE's cvIncreaseBDF /
+// cvDecreaseBDF).  Out of line: order changes are rare.
+template <class MT, class LinT>
+__device__ __noinline__ void bdf_adjust_order(unsigned off, int dq, int lane) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    const int q = S.q;
+    if (q == 2 && dq != 1) return;
+    double* l = S.l;
+    for (int j = 0; j <= cv::QMAX; ++j) l[j] = 0.0;
+    l[2] = 1.0;
+    if (dq == 1) {
+        double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = S.hscale;
         for (int j = 1; j < q; ++j) {
-            hsum += tau[j + 1];
-            const double xi = hsum / hscale;
+            hsum += S.tau[j + 1];
+            const double xi = hsum / S.hscale;
             prod *= xi;
             alpha0 -= 1.0 / (j + 1);
             alpha1 += 1.0 / xi;
@@ -206,450 +189,349 @@ struct WarpBdf {
             xiold = xi;
         }
         const double A1 = (-alpha0 - alpha1) / prod;
-        const double* acs = zn(indx_acor);
-        double* zl = zn(L);
-        double col[NS];
+        const int L = S.L, ia = S.indx_acor;
 #pragma unroll
-        for (int s = 0; s < NS; ++s) { col[s] = A1 * acs[32 * s]; zl[32 * s] = col[s]; }
-        for (int j = 2; j <= q; ++j) {
-            double* z = zn(j);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] += l[j] * col[s];
+        for (int s = 0; s < MT::NS; ++s) {
+            const int i = lane + 32 * s;
+            const double col = A1 * w->zn[ia][i];
+            w->zn[L][i] = col;
+            for (int j = 2; j <= q; ++j) w->zn[j][i] += l[j] * col;
         }
-    }
-    __device__ __forceinline__ void decrease_bdf() {
-        double* l = sm->l;
-        const double* tau = sm->tau;
-        for (int j = 0; j <= cv::QMAX; ++j) l[j] = 0.0;
-        l[2] = 1.0;
+    } else if (dq == -1) {
         double hsum = 0.0;
         for (int j = 1; j <= q - 2; ++j) {
-            hsum += tau[j];
-            const double xi = hsum / hscale;
+            hsum += S.tau[j];
+            const double xi = hsum / S.hscale;
             for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
         }
-        const double* zq = zn(q);
+#pragma unroll
+        for (int s = 0; s < MT::NS; ++s) {
+            const int i = lane + 32 * s;
+            const double zq = w->zn[q][i];
+            for (int j = 2; j < q; ++j) w->zn[j][i] += -l[j] * zq;
+        }
+    }
+}
+
+// BDF coefficients l[0..q], error constants tq[1..5], gamma (CVODE's cvSet,
+// cvSetBDF, cvSetTqBDF).
+template <class MT, class LinT>
+__device__ __noinline__ void bdf_set_coeffs(unsigned off) {
+    BdfState& S = wsm<MT, LinT>(off)->st;
+    double* l = S.l;
+    double* tq = S.tq;
+    const double* tau = S.tau;
+    const int q = S.q;
+    const double h = S.h;
+    l[0] = l[1] = 1.0;
+    double xi_inv = 1.0, xistar_inv = 1.0;
+    for (int j = 2; j <= cv::QMAX; ++j) l[j] = 0.0;
+    double alpha0 = -1.0, alpha0_hat = -1.0, hsum = h;
+    if (q > 1) {
         for (int j = 2; j < q; ++j) {
-            double* z = zn(j);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] += -l[j] * zq[32 * s];
+            hsum += tau[j - 1];
+            xi_inv = h / hsum;
+            alpha0 -= 1.0 / j;
+            for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
         }
+        alpha0 -= 1.0 / q;
+        xistar_inv = -l[1] - alpha0;
+        hsum += tau[q - 1];
+        xi_inv = h / hsum;
+        alpha0_hat = -l[1] - xi_inv;
+        for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
     }
-    __device__ __forceinline__ void adjust_order(int dq) {
-        if (q == 2 && dq != 1) return;
-        if (dq == 1) increase_bdf();
-        else if (dq == -1) decrease_bdf();
-    }
-    __device__ __forceinline__ void adjust_params() {
-        if (qprime != q) {
-            adjust_order(qprime - q);
-            q = qprime;
-            L = q + 1;
-            qwait = L;
-        }
-        rescale();
-    }
-
-    // --------------------------------------------------------- coefficients
-    __device__ __forceinline__ void set_coeffs() {
-        double* l = sm->l;
-        double* tq = sm->tq;
-        const double* tau = sm->tau;
-        l[0] = l[1] = 1.0;
-        double xi_inv = 1.0, xistar_inv = 1.0;
-        for (int j = 2; j <= cv::QMAX; ++j) l[j] = 0.0;
-        double alpha0 = -1.0, alpha0_hat = -1.0, hsum = h;
+    const double A1 = 1.0 - alpha0_hat + alpha0;
+    const double A2 = 1.0 + q * A1;
+    tq[2] = fabs(A1 / (alpha0 * A2));
+    tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
+    if (S.qwait == 1) {
         if (q > 1) {
-            for (int j = 2; j < q; ++j) {
-                hsum += tau[j - 1];
-                xi_inv = h / hsum;
-                alpha0 -= 1.0 / j;
-                for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
-            }
-            alpha0 -= 1.0 / q;
-            xistar_inv = -l[1] - alpha0;
-            hsum += tau[q - 1];
-            xi_inv = h / hsum;
-            alpha0_hat = -l[1] - xi_inv;
-            for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
-        }
-        // error constants (CVODE's cvSetTqBDF)
-        const double A1 = 1.0 - alpha0_hat + alpha0;
-        const double A2 = 1.0 + q * A1;
-        tq[2] = fabs(A1 / (alpha0 * A2));
-        tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
-        if (qwait == 1) {
-            if (q > 1) {
-                const double C = xistar_inv / l[q];
-                const double A3 = alpha0 + 1.0 / q;
-                const double A4 = alpha0_hat + xi_inv;
-                const double Cpinv = (1.0 - A4 + A3) / A3;
-                tq[1] = fabs(C * Cpinv);
-            } else {
-                tq[1] = 1.0;
-            }
-            hsum += tau[q];
-            xi_inv = h / hsum;
-            const double A5 = alpha0 - 1.0 / (q + 1);
-            const double A6 = alpha0_hat - xi_inv;
-            const double Cppinv = (1.0 - A6 + A5) / A2;
-            tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
-        }
-        tq[4] = cv::NLSCOEF / tq[2];
-        rl1 = 1.0 / l[1];
-        gamma = h * rl1;
-        if (nst == 0) gammap = gamma;
-        gamrat = (nst > 0) ? gamma / gammap : 1.0;
-    }
-
-    // -------------------------------------------------------------- Newton
-    // residual: y = zn0 + ycor; ftemp = f(y); res = rl1*zn1 + ycor - gamma*ftemp
-    __device__ __forceinline__ void nls_residual(const double (&ycor)[NS], double (&res)[NS]) {
-        const double* z0 = zn(0);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) y[s] = z0[32 * s] + ycor[s];
-        rhs(y, ftemp);
-        const double* z1 = zn(1);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            res[s] = rl1 * z1[32 * s] + ycor[s];
-            res[s] = -gamma * ftemp[s] + res[s];
-        }
-    }
-    // J reuse decision, M = I - gamma J, LU.  Returns nonzero if singular.
-    __device__ __forceinline__ int ls_setup(int cf) {
-        constexpr int LDA = MT::LDA;
-        const double dgamma = fabs(gamma / gammap - 1.0);
-        const bool jbad = (nst == 0) || (nst >= nstlj + cv::MSBJ) ||
-                          ((cf == cv::FAIL_BAD_J) && (dgamma < cv::DGMAX_JBAD)) || (cf == cv::FAIL_OTHER);
-        LinT* A = sm->A;
-        LinT* J = wg->savedJ;
-        if (!jbad) {
-            jcur = 0;
-            for (int i = 0; i < N; ++i)
-                for (int j = lane; j < N; j += 32) A[i * LDA + j] = J[i * N + j];
+            const double C = xistar_inv / l[q];
+            const double A3 = alpha0 + 1.0 / q;
+            const double A4 = alpha0_hat + xi_inv;
+            const double Cpinv = (1.0 - A4 + A3) / A3;
+            tq[1] = fabs(C * Cpinv);
         } else {
-            cnt.nje++;
-            nstlj = nst;
-            jcur = 1;
-            const long long tj = tick();
-            Vec<NS> yy;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) yy.v[s] = y[s];
-            warp_jac<MT, LinT>(P, yy, A, &sm->chem, &wg->js, lane);
-            tock(PH_JAC, tj);
-            for (int i = 0; i < N; ++i)
-                for (int j = lane; j < N; j += 32) J[i * N + j] = A[i * LDA + j];
+            tq[1] = 1.0;
         }
-        __syncwarp();
-        const LinT mg = (LinT)(-gamma);
+        hsum += tau[q];
+        xi_inv = h / hsum;
+        const double A5 = alpha0 - 1.0 / (q + 1);
+        const double A6 = alpha0_hat - xi_inv;
+        const double Cppinv = (1.0 - A6 + A5) / A2;
+        tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+    }
+    tq[4] = cv::NLSCOEF / tq[2];
+    S.rl1 = 1.0 / l[1];
+    S.gamma = h * S.rl1;
+    if (S.nst == 0) S.gammap = S.gamma;
+    S.gamrat = (S.nst > 0) ? S.gamma / S.gammap : 1.0;
+}
+
+// Linear-solver setup (CVODE's cvNlsLSetup + cvLsSetup): Jacobian reuse
+// decision, M = I - gamma J, LU.  Returns nonzero if M is singular.
+template <class MT, class LinT>
+__device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, WarpGlobal<MT, LinT>* wg, int jbad_in,
+                                         int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    if (jbad_in) S.convfail = cv::FAIL_BAD_J;
+    const int cf = S.convfail;
+    const double dgamma = fabs(S.gamma / S.gammap - 1.0);
+    const bool jbad = (S.nst == 0) || (S.nst >= S.nstlj + cv::MSBJ) ||
+                      ((cf == cv::FAIL_BAD_J) && (dgamma < cv::DGMAX_JBAD)) || (cf == cv::FAIL_OTHER);
+    LinT* A = w->A;
+    LinT* J = wg->savedJ;
+    if (!jbad) {
+        S.jcur = 0;
+#pragma unroll 1
         for (int i = 0; i < N; ++i)
-            for (int j = lane; j < N; j += 32) {
-                LinT v = mg * A[i * LDA + j];
-                if (i == j) v += LinT(1);
-                A[i * LDA + j] = v;
-            }
-        __syncwarp();
-        lu_dirty = 1;
-        const long long tl = tick();
-        const int r = warp_lu<MT, LinT>(A, sm->perm, sm->dinv, lane);
-        tock(PH_LU, tl);
-        return r;
+            for (int j = lane; j < N; j += 32) A[i * LDA + j] = J[i * N + j];
+    } else {
+        S.cnt[C_NJE]++;
+        S.nstlj = S.nst;
+        S.jcur = 1;
+        const long long tj = ph_tick(S);
+        warp_jac<MT, LinT>(S.P, yv, smem_off(A), smem_off(&w->chem), &wg->js, lane);
+        ph_tock(S, PH_JAC, tj, lane);
+#pragma unroll 1
+        for (int i = 0; i < N; ++i)
+            for (int j = lane; j < N; j += 32) J[i * N + j] = A[i * LDA + j];
     }
-    __device__ __forceinline__ int nls_lsetup(int jbad) {
-        if (jbad) convfail = cv::FAIL_BAD_J;
-        const int ret = ls_setup(convfail);
-        cnt.nsetups++;
-        gamrat = 1.0;
-        gammap = gamma;
-        crate = 1.0;
-        nstlp = nst;
-        return ret ? cv::CONV_RECVR : 0;
-    }
-    // r = b - (I - gammap J) x in FP64, J from the saved Jacobian.
-    __device__ __forceinline__ void refine_residual(const double (&b)[NS], const double (&x)[NS],
-                                                 double (&r)[NS]) {
+    __syncwarp();
+    const LinT mg = (LinT)(-S.gamma);
+#pragma unroll 1
+    for (int i = 0; i < N; ++i)
+        for (int j = lane; j < N; j += 32) {
+            LinT v = mg * A[i * LDA + j];
+            if (i == j) v += LinT(1);
+            A[i * LDA + j] = v;
+        }
+    __syncwarp();
+    S.lu_dirty = 1;
+    const long long tl = ph_tick(S);
+    const int r = warp_lu<MT, LinT>(smem_off(A), smem_off(w->perm), smem_off(w->dinv), lane);
+    ph_tock(S, PH_LU, tl, lane);
+    S.cnt[C_NSETUPS]++;
+    S.gamrat = 1.0;
+    S.gammap = S.gamma;
+    S.crate = 1.0;
+    S.nstlp = S.nst;
+    return r;
+}
+
+// Newton correction solve: M delta = b, then CVODE's 2/(1+gamrat) scaling;
+// optional FP64 refinement sweep against the saved Jacobian.
+template <class MT, class LinT>
+__device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], const WarpGlobal<MT, LinT>* wg,
+                                          int lane) {
+    constexpr int N = MT::N, NS = MT::NS;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    const long long t0 = ph_tick(S);
+    Vec<NS> a;
 #pragma unroll
-        for (int s = 0; s < NS; ++s) r[s] = b[s] - x[s];
+    for (int s = 0; s < NS; ++s) a.v[s] = b[s];
+    Vec<NS> x = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), smem_off(w->dinv), a, lane);
+    if (S.refine && sizeof(LinT) < sizeof(double)) {
+        // r = b - (I - gammap J) x in FP64; x += M^{-1} r
+        Vec<NS> r;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) r.v[s] = a.v[s] - x.v[s];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + 32 * s;
             double acc = 0.0;
 #pragma unroll 1
             for (int j = 0; j < N; ++j) {
-                const double xj = __shfl_sync(kFull, x[j >> 5 < NS ? j >> 5 : 0], j & 31);
+                const double xj = __shfl_sync(kFull, (NS == 1 || j < 32) ? x.v[0] : x.v[NS - 1], j & 31);
                 if (i < N) acc += (double)wg->savedJ[i * N + j] * xj;
             }
-            if (i < N) r[s] += gammap * acc;
+            if (i < N) r.v[s] += S.gammap * acc;
         }
+        const Vec<NS> d = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), smem_off(w->dinv), r, lane);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) x.v[s] += d.v[s];
     }
-    __device__ __forceinline__ void ls_solve(double (&b)[NS]) {
-        if (refine && sizeof(LinT) < sizeof(double)) {
-            double b0[NS];
+    const double gamrat = S.gamrat;
+    const double sc = (gamrat != 1.0) ? 2.0 / (1.0 + gamrat) : 1.0;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) b0[s] = b[s];
-            lu_solve(b);
-            double r[NS];
-            refine_residual(b0, b, r);
-            lu_solve(r);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) b[s] += r[s];
-        } else {
-            lu_solve(b);
-        }
-        if (gamrat != 1.0) {
-            const double sc = 2.0 / (1.0 + gamrat);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) b[s] *= sc;
-        }
+    for (int s = 0; s < NS; ++s) b[s] = (gamrat != 1.0) ? x.v[s] * sc : x.v[s];
+    ph_tock(S, PH_SOLVE, t0, lane);
+}
+
+// Step-size / order selection after an accepted step (CVODE's
+// cvPrepareNextStep, cvComputeEtaqm1/qp1, cvChooseEta, cvSetEta).
+template <class MT, class LinT>
+__device__ __noinline__ void bdf_prepare_next_step(unsigned off, double dsm, const Vec<MT::NS> acv,
+                                                   const Vec<MT::NS> ewv, int lane) {
+    constexpr int NS = MT::NS;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    const int q = S.q, L = S.L;
+    if (S.etamax == 1.0) {
+        if (S.qwait < 2) S.qwait = 2;
+        S.qprime = q;
+        S.hprime = S.h;
+        S.eta = 1.0;
+        return;
     }
-    __device__ __forceinline__ int nls_solve(int call_setup) {
-        int jbad = 0, ret = 0;
-#pragma unroll 1
-        for (int attempt = 0; attempt < 4; ++attempt) {
-            nls_residual(acor, delta);
-            if (call_setup) {
-                ret = nls_lsetup(jbad);
-                if (ret) break;
-            }
-            double delp = 0.0;
-            ret = 0;
-#pragma unroll 1
-            for (int m = 0;; ++m) {
-                cnt.nni++;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) delta[s] = -delta[s];
-                ls_solve(delta);
-#pragma unroll
-                for (int s = 0; s < NS; ++s) acor[s] += delta[s];
-                const double del = wrms(delta);
-                if (m > 0) crate = fmax(cv::CRDOWN * crate, del / delp);
-                const double dcon = del * fmin(1.0, crate) / sm->tq[4];
-                if (dcon <= 1.0) {
-                    acnrm = (m == 0) ? del : wrms(acor);
-                    jcur = 0;
-                    return 0;
-                }
-                if (m >= 1 && del > cv::RDIV * delp) { ret = cv::CONV_RECVR; break; }
-                delp = del;
-                if (m + 1 >= cv::NLS_MAXCOR) { ret = cv::CONV_RECVR; break; }
-                nls_residual(acor, delta);
-            }
-            if (ret == cv::CONV_RECVR && !jcur) {
-                call_setup = 1;
-                jbad = 1;
-#pragma unroll
-                for (int s = 0; s < NS; ++s) acor[s] = 0.0;
-                continue;
-            }
-            break;
-        }
-        return ret;
-    }
-    __device__ __forceinline__ int nls(int nflag) {
-        convfail = ((nflag == cv::FIRST_CALL) || (nflag == cv::PREV_ERR_FAIL)) ? cv::NO_FAILURES : cv::FAIL_OTHER;
-        const int call_setup = (nflag == cv::PREV_CONV_FAIL) || (nflag == cv::PREV_ERR_FAIL) || (nst == 0) ||
-                               (nst >= nstlp + cv::MSBP) || (fabs(gamrat - 1.0) > cv::DGMAX_LSETUP);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) acor[s] = 0.0;
-        return nls_solve(call_setup);
-    }
-    __device__ __forceinline__ int handle_nflag(int& nflag, double saved_t, int& ncf) {
-        if (nflag == 0) return cv::DO_ERROR_TEST;
-        cnt.ncfn++;
-        restore(saved_t);
-        ncf++;
-        etamax = 1.0;
-        if (ncf == cv::MXNCF) return cv::CV_CONV_FAILURE;
-        eta = cv::ETACF;
-        nflag = cv::PREV_CONV_FAIL;
-        rescale();
-        return cv::PREDICT_AGAIN;
-    }
-    __device__ __forceinline__ int do_error_test(int& nflag, double saved_t, int& nef, double& dsm) {
-        dsm = acnrm * sm->tq[2];
-        if (dsm <= 1.0) return 0;
-        nef++;
-        cnt.netf++;
-        nflag = cv::PREV_ERR_FAIL;
-        restore(saved_t);
-        if (nef == cv::MXNEF) return cv::CV_ERR_FAILURE;
-        etamax = 1.0;
-        if (nef <= cv::MXNEF1) {
-            eta = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / L) + cv::ADDON);
-            eta = fmax(cv::ETAMIN, eta);
-            if (nef >= cv::SMALL_NEF) eta = fmin(eta, cv::ETAMXF);
-            rescale();
-            return cv::TRY_AGAIN;
-        }
+    S.etaq = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / L) + cv::ADDON);
+    double eta;
+    int qprime = q;
+    if (S.qwait != 0) {
+        eta = S.etaq;
+    } else {
+        S.qwait = 2;
+        double etaqm1 = 0.0, etaqp1 = 0.0;
         if (q > 1) {
-            eta = cv::ETAMIN;
-            adjust_order(-1);
-            L = q;
-            q--;
-            qwait = L;
-            rescale();
-            return cv::TRY_AGAIN;
-        }
-        eta = cv::ETAMIN;
-        h *= eta;
-        hscale = h;
-        qwait = cv::LONG_WAIT;
-        rhs_zn0(tempv);
-        double* z1 = zn(1);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) z1[32 * s] = h * tempv[s];
-        return cv::TRY_AGAIN;
-    }
-    __device__ __forceinline__ void complete_step() {
-        double* tau = sm->tau;
-        const double* l = sm->l;
-        nst++;
-        hu = h;
-        for (int i = q; i >= 2; --i) tau[i] = tau[i - 1];
-        if (q == 1 && nst > 1) tau[2] = tau[1];
-        tau[1] = h;
-#pragma unroll 1
-        for (int j = 0; j <= q; ++j) {
-            double* z = zn(j);
-            const double lj = l[j];
-#pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] += lj * acor[s];
-        }
-        qwait--;
-        if (qwait == 1 && q != qmax) {
-            double* zm = zn(qmax);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) zm[32 * s] = acor[s];
-            saved_tq5 = sm->tq[5];
-            indx_acor = qmax;
-        }
-    }
-    __device__ __forceinline__ void set_eta() {
-        if (eta < cv::THRESH) {
-            eta = 1.0;
-            hprime = h;
-        } else {
-            eta = fmin(eta, etamax);
-            hprime = h * eta;
-        }
-    }
-    __device__ __forceinline__ void prepare_next_step(double dsm) {
-        if (etamax == 1.0) {
-            if (qwait < 2) qwait = 2;
-            qprime = q;
-            hprime = h;
-            eta = 1.0;
-            return;
-        }
-        etaq = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / L) + cv::ADDON);
-        if (qwait != 0) {
-            eta = etaq;
-            qprime = q;
-            set_eta();
-            return;
-        }
-        qwait = 2;
-        // eta at order q-1
-        etaqm1 = 0.0;
-        if (q > 1) {
-            const double ddn = wrms_zn(q) * sm->tq[1];
+            const double ddn = wrms_zn<MT, LinT>(w, q, ewv.v, lane) * S.tq[1];
             etaqm1 = 1.0 / (pow(cv::BIAS1 * ddn, 1.0 / q) + cv::ADDON);
         }
-        // eta at order q+1
-        etaqp1 = 0.0;
-        if (q != qmax && saved_tq5 != 0.0) {
-            const double cquot = (sm->tq[5] / saved_tq5) * pow(h / sm->tau[2], (double)L);
-            const double* zm = zn(qmax);
+        if (q != S.qmax && S.saved_tq5 != 0.0) {
+            const double cquot = (S.tq[5] / S.saved_tq5) * pow(S.h / S.tau[2], (double)L);
+            double tmp[NS];
 #pragma unroll
-            for (int s = 0; s < NS; ++s) tempv[s] = acor[s] - cquot * zm[32 * s];
-            const double dup = wrms(tempv) * sm->tq[3];
+            for (int s = 0; s < NS; ++s) tmp[s] = acv.v[s] - cquot * w->zn[S.qmax][lane + 32 * s];
+            const double dup = wrms_v<NS>(tmp, ewv.v, MT::N) * S.tq[3];
             etaqp1 = 1.0 / (pow(cv::BIAS3 * dup, 1.0 / (L + 1)) + cv::ADDON);
         }
-        // choose
+        S.etaqm1 = etaqm1;
+        S.etaqp1 = etaqp1;
+        const double etaq = S.etaq;
         const double etam = fmax(etaqm1, fmax(etaq, etaqp1));
         if (etam < cv::THRESH) {
             eta = 1.0;
-            qprime = q;
         } else if (etam == etaqm1) {
             eta = etaqm1;
             qprime = q - 1;
         } else if (etam == etaq) {
             eta = etaq;
-            qprime = q;
         } else {
             eta = etaqp1;
             qprime = q + 1;
-            double* zm = zn(qmax);
 #pragma unroll
-            for (int s = 0; s < NS; ++s) zm[32 * s] = acor[s];
+            for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + 32 * s] = acv.v[s];
         }
-        set_eta();
     }
-    // One internal step.  Returns 0 or a negative CVODE code.
-    __device__ __forceinline__ int step() {
-        const double saved_t = tn;
-        int ncf = 0, nef = 0, nflag = cv::FIRST_CALL;
-        double dsm = 0.0;
-        if (nst > 0 && hprime != h) adjust_params();
-#pragma unroll 1
-        for (int guard = 0; guard < 64; ++guard) {
-            predict();
-            set_coeffs();
-            nflag = nls(nflag);
-            const int kflag = handle_nflag(nflag, saved_t, ncf);
-            if (kflag == cv::PREDICT_AGAIN) continue;
-            if (kflag != cv::DO_ERROR_TEST) return kflag;
-            const int eflag = do_error_test(nflag, saved_t, nef, dsm);
-            if (eflag == cv::TRY_AGAIN) continue;
-            if (eflag != 0) return eflag;
-            complete_step();
-            prepare_next_step(dsm);
-            etamax = (nst <= cv::SMALL_NST) ? cv::ETAMX2 : cv::ETAMX3;
-            const double t2 = sm->tq[2];
-#pragma unroll
-            for (int s = 0; s < NS; ++s) acor[s] *= t2;
-            return 0;
-        }
-        return cv::CV_CONV_FAILURE;   // unreachable: ncf < 10 and nef < 7 bound the attempts
+    S.qprime = qprime;
+    // cvSetEta
+    if (eta < cv::THRESH) {
+        eta = 1.0;
+        S.hprime = S.h;
+    } else {
+        eta = fmin(eta, S.etamax);
+        S.hprime = S.h * eta;
     }
+    S.eta = eta;
+}
 
-    // ------------------------------------------------------------ initial h
-    __device__ __forceinline__ int hin(double tout, double& h0) {
-        const double tdiff = tout - tn;
-        if (tdiff == 0.0) return cv::CV_TOO_CLOSE;
-        const int sign = (tdiff > 0.0) ? 1 : -1;
-        const double tdist = fabs(tdiff);
-        const double tround = cv::UROUND * fmax(fabs(tn), fabs(tout));
-        if (tdist < 2.0 * tround) return cv::CV_TOO_CLOSE;
-        const double hlb = cv::HLB_FACTOR * tround;
-        // upper bound from |y0| / |y0'| (CVODE's cvUpperBoundH0)
-        const double* z0 = zn(0);
-        const double* z1 = zn(1);
-        double r = 0.0;
+// Failed error test: counters, restore and the new step (CVODE's
+// cvDoErrorTest failure branch).  Returns TRY_AGAIN or CV_ERR_FAILURE.
+template <class MT, class LinT>
+__device__ __noinline__ int bdf_error_fail(unsigned off, double dsm, double saved_t, int nef, int lane) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    S.cnt[C_NETF]++;
+    S.tn = saved_t;
+    bdf_pascal<MT, LinT>(off, lane, false);
+    if (nef == cv::MXNEF) return cv::CV_ERR_FAILURE;
+    S.etamax = 1.0;
+    if (nef <= cv::MXNEF1) {
+        double eta = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / S.L) + cv::ADDON);
+        eta = fmax(cv::ETAMIN, eta);
+        if (nef >= cv::SMALL_NEF) eta = fmin(eta, cv::ETAMXF);
+        S.eta = eta;
+        bdf_rescale<MT, LinT>(off, lane);
+        return cv::TRY_AGAIN;
+    }
+    if (S.q > 1) {
+        S.eta = cv::ETAMIN;
+        bdf_adjust_order<MT, LinT>(off, -1, lane);
+        S.L = S.q;
+        S.q--;
+        S.qwait = S.L;
+        bdf_rescale<MT, LinT>(off, lane);
+        return cv::TRY_AGAIN;
+    }
+    S.eta = cv::ETAMIN;
+    S.h *= S.eta;
+    S.hscale = S.h;
+    S.qwait = cv::LONG_WAIT;
+    double z0[MT::NS], f[MT::NS];
 #pragma unroll
-        for (int s = 0; s < NS; ++s)
-            if (valid(s)) {
-                const double den = cv::HUB_FACTOR * fabs(z0[32 * s]) + 1.0 / ewt[s];
-                r = fmax(r, fabs(z1[32 * s]) / den);
-            }
-        const double hub_inv = warp_max(r);
-        double hub = cv::HUB_FACTOR * tdist;
-        if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
-        double hg = sqrt(hlb * hub);
-        if (hub < hlb) { h0 = sign * hg; return 0; }
-        double hnew = hg;
+    for (int s = 0; s < MT::NS; ++s) z0[s] = w->zn[0][lane + 32 * s];
+    bdf_rhs<MT, LinT>(off, z0, f, lane);
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) w->zn[1][lane + 32 * s] = S.h * f[s];
+    return cv::TRY_AGAIN;
+}
+
+// Initial state and step (CVode's first call: ewt, f(y0), cvHin).  Returns 0 or
+// a CVODE code.  Out of line: once per cell.
+template <class MT, class LinT>
+__device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double t0, double tout, int lane) {
+    constexpr int NS = MT::NS, N = MT::N;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
 #pragma unroll 1
+    for (int j = 0; j <= cv::QMAX; ++j)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) w->zn[j][lane + 32 * s] = (j == 0 && valid_el<NS>(lane, s, N)) ? y0.v[s] : 0.0;
+    for (int j = 0; j < 8; ++j) S.l[j] = S.tq[j] = S.tau[j] = 0.0;
+    for (int j = 0; j < 7; ++j) S.cnt[j] = 0;
+    S.tn = t0;
+    S.q = 1; S.L = 2; S.qwait = 2; S.qprime = 1;
+    S.etamax = cv::ETAMX1;
+    S.indx_acor = S.qmax;
+    S.crate = 1.0;
+    S.h = S.hprime = S.hscale = S.eta = S.hu = S.saved_tq5 = 0.0;
+    S.gamma = S.gammap = S.gamrat = S.rl1 = S.acnrm = S.etaq = S.etaqm1 = S.etaqp1 = 0.0;
+    S.jcur = 0; S.convfail = 0; S.nst = S.nstlp = S.nstlj = 0; S.nstloc = 0;
+    double ewt[NS], z0[NS], z1[NS], y[NS], tmp[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        z0[s] = valid_el<NS>(lane, s, N) ? y0.v[s] : 0.0;
+        ewt[s] = valid_el<NS>(lane, s, N) ? 1.0 / (S.rtol * fabs(z0[s]) + S.atol) : 0.0;
+    }
+    bdf_rhs<MT, LinT>(off, z0, z1, lane);
+#pragma unroll
+    for (int s = 0; s < NS; ++s) if (!valid_el<NS>(lane, s, N)) z1[s] = 0.0;
+    // ---- cvHin
+    const double tdiff = tout - t0;
+    if (tdiff == 0.0) return cv::CV_TOO_CLOSE;
+    const int sign = (tdiff > 0.0) ? 1 : -1;
+    const double tdist = fabs(tdiff);
+    const double tround = cv::UROUND * fmax(fabs(t0), fabs(tout));
+    if (tdist < 2.0 * tround) return cv::CV_TOO_CLOSE;
+    const double hlb = cv::HLB_FACTOR * tround;
+    double r = 0.0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        if (valid_el<NS>(lane, s, N)) {
+            const double den = cv::HUB_FACTOR * fabs(z0[s]) + 1.0 / ewt[s];
+            r = fmax(r, fabs(z1[s]) / den);
+        }
+    const double hub_inv = warp_max(r);
+    double hub = cv::HUB_FACTOR * tdist;
+    if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
+    double hg = sqrt(hlb * hub);
+    double h0;
+    if (hub < hlb) {
+        h0 = sign * hg;
+    } else {
+        double hnew = hg;
         for (int count1 = 1; count1 <= cv::MAX_HIN_ITERS; ++count1) {
-            // ||y''|| estimate from one RHS evaluation (cvYddNorm)
             const double hgs = hg * sign;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) y[s] = hgs * z1[32 * s] + z0[32 * s];
-            rhs(y, tempv);
+            for (int s = 0; s < NS; ++s) y[s] = hgs * z1[s] + z0[s];
+            bdf_rhs<MT, LinT>(off, y, tmp, lane);
             const double ih = 1.0 / hgs;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) tempv[s] = (tempv[s] - z1[32 * s]) * ih;
-            const double yddnrm = wrms(tempv);
+            for (int s = 0; s < NS; ++s) tmp[s] = (tmp[s] - z1[s]) * ih;
+            const double yddnrm = wrms_v<NS>(tmp, ewt, N);
             hnew = (yddnrm * hub * hub > 2.0) ? sqrt(2.0 / yddnrm) : sqrt(hg * hub);
             if (count1 == cv::MAX_HIN_ITERS) break;
             const double hrat = hnew / hg;
@@ -661,159 +543,260 @@ struct WarpBdf {
         if (hh < hlb) hh = hlb;
         if (hh > hub) hh = hub;
         h0 = sign * hh;
-        return 0;
     }
+    S.h = h0;
+    S.hscale = h0;
+    S.hprime = h0;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) w->zn[1][lane + 32 * s] = z1[s] * h0;
+    return 0;
+}
 
-    // ---------------------------------------------------------------- driver
-    // Set up y0 at t0 toward tout: ewt, f(y0), initial step (CVode's first-call
-    // path).  Returns 0 or a CVODE code.
-    __device__ __forceinline__ int begin(const double (&y0)[NS], double t0, double tout) {
-        cnt = CellCounters{0, 0, 0, 0, 0, 0, 0};
-        for (int j = 0; j <= cv::QMAX; ++j) {
-            double* z = zn(j);
+// Output: y(tout) by interpolation on success (CVodeGetDky), else the last
+// accepted state.
+template <class MT, class LinT>
+__device__ __noinline__ Vec<MT::NS> bdf_finish(unsigned off, int status, double tout, int lane) {
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    Vec<MT::NS> out;
+    if (status == 0) {
+        const double s_ = (tout - S.tn) / S.h;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] = (j == 0 && valid(s)) ? y0[s] : 0.0;
-        }
-        for (int j = 0; j < 8; ++j) sm->l[j] = sm->tq[j] = sm->tau[j] = 0.0;
+        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[S.q][lane + 32 * s];
+        for (int j = S.q - 1; j >= 0; --j)
 #pragma unroll
-        for (int s = 0; s < NS; ++s) acor[s] = tempv[s] = ftemp[s] = y[s] = delta[s] = 0.0;
-        tn = t0;
-        q = 1; L = 2; qwait = L; qprime = 1;
-        etamax = cv::ETAMX1;
-        indx_acor = qmax;
-        crate = 1.0;
-        h = hprime = hscale = eta = hu = saved_tq5 = 0.0;
-        gamma = gammap = gamrat = rl1 = acnrm = etaq = etaqm1 = etaqp1 = 0.0;
-        jcur = 0; convfail = 0; nst = nstlp = nstlj = 0; nstloc = 0;
-        set_ewt_zn0();
-        double f0[NS];
-        rhs_zn0(f0);
-        double* z1 = zn(1);
+            for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[j][lane + 32 * s] + s_ * out.v[s];
+    } else {
 #pragma unroll
-        for (int s = 0; s < NS; ++s) z1[32 * s] = valid(s) ? f0[s] : 0.0;
-        double h0 = 0.0;
-        const int status = hin(tout, h0);
-        if (status == 0) {
-            h = h0;
-            hscale = h0;
-            hprime = h0;
-#pragma unroll
-            for (int s = 0; s < NS; ++s) z1[32 * s] *= h0;
-        }
-        return status;
+        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[0][lane + 32 * s];
     }
-    // Take up to max_new internal steps toward tout.  Sets done when tout is
-    // reached or a step failed; returns 0 or a negative CVODE code.
-    __device__ __forceinline__ int advance(double tout, int max_new, bool& done) {
-        done = false;
+    S.cnt[C_NST] = S.nst;
+    return out;
+}
+
+// Take up to max_new internal steps toward tout (CVode's main loop with
+// cvStep inlined).  Sets done when tout is reached or a step failed; returns 0
+// or a negative CVODE code.
+template <class MT, class LinT>
+__device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* wg, double tout, int max_new,
+                                           bool& done, int lane) {
+    constexpr int NS = MT::NS, N = MT::N;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    BdfState& S = w->st;
+    double ewt[NS], acor[NS], y[NS], ftemp[NS], delta[NS];
+    done = false;
 #pragma unroll 1
-        for (int k = 0; k < max_new; ++k) {
-            if (nst > 0) set_ewt_zn0();
-            if (nstloc >= max_steps) { done = true; return cv::CV_TOO_MUCH_WORK; }
-            const double tolsf = cv::UROUND * wrms_zn(0);
-            if (tolsf > 1.0) { done = true; return cv::CV_TOO_MUCH_ACC; }
-            const int kflag = step();
-            if (kflag != 0) { done = true; return kflag; }
-            nstloc++;
-            if ((tn - tout) * h >= 0.0) { done = true; return 0; }
-        }
-        return 0;
-    }
-    // Output: y(tout) by interpolation on success (CVodeGetDky), else the last
-    // accepted state.
-    __device__ __forceinline__ void finish(int status, double tout, double (&yout)[NS]) {
-        if (status == 0) {
-            const double s_ = (tout - tn) / h;
-            const double* zq = zn(q);
+    for (int k = 0; k < max_new; ++k) {
+        // ---- CVode loop: error weights, work limit, accuracy check
 #pragma unroll
-            for (int s = 0; s < NS; ++s) yout[s] = zq[32 * s];
-#pragma unroll 1
-            for (int j = q - 1; j >= 0; --j) {
-                const double* z = zn(j);
-#pragma unroll
-                for (int s = 0; s < NS; ++s) yout[s] = z[32 * s] + s_ * yout[s];
+        for (int s = 0; s < NS; ++s)
+            ewt[s] = valid_el<NS>(lane, s, N) ? 1.0 / (S.rtol * fabs(w->zn[0][lane + 32 * s]) + S.atol) : 0.0;
+        if (S.nstloc >= S.max_steps) { done = true; return cv::CV_TOO_MUCH_WORK; }
+        if (cv::UROUND * wrms_zn<MT, LinT>(w, 0, ewt, lane) > 1.0) { done = true; return cv::CV_TOO_MUCH_ACC; }
+        // ---- cvStep
+        const double saved_t = S.tn;
+        int ncf = 0, nef = 0, nflag = cv::FIRST_CALL;
+        double dsm = 0.0;
+        int kflag = 0;
+        if (S.nst > 0 && S.hprime != S.h) {
+            if (S.qprime != S.q) {
+                bdf_adjust_order<MT, LinT>(off, S.qprime - S.q, lane);
+                S.q = S.qprime;
+                S.L = S.q + 1;
+                S.qwait = S.L;
             }
-        } else {
-            const double* z0 = zn(0);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) yout[s] = z0[32 * s];
+            bdf_rescale<MT, LinT>(off, lane);
         }
-        cnt.nst = nst;
+#pragma unroll 1
+        for (int guard = 0; guard < 64; ++guard) {
+            S.tn += S.h;
+            bdf_pascal<MT, LinT>(off, lane, true);
+            bdf_set_coeffs<MT, LinT>(off);
+            // ---- cvNls: modified Newton
+            S.convfail = ((nflag == cv::FIRST_CALL) || (nflag == cv::PREV_ERR_FAIL)) ? cv::NO_FAILURES : cv::FAIL_OTHER;
+            int call_setup = (nflag == cv::PREV_CONV_FAIL) || (nflag == cv::PREV_ERR_FAIL) || (S.nst == 0) ||
+                             (S.nst >= S.nstlp + cv::MSBP) || (fabs(S.gamrat - 1.0) > cv::DGMAX_LSETUP);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) acor[s] = 0.0;
+            int jbad = 0, ret = 0;
+#pragma unroll 1
+            for (int attempt = 0; attempt < 4; ++attempt) {
+                // residual at ycor = acor
+#pragma unroll
+                for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + 32 * s] + acor[s];
+                bdf_rhs<MT, LinT>(off, y, ftemp, lane);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + 32 * s] + acor[s]);
+                if (call_setup) {
+                    Vec<NS> yv;
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) yv.v[s] = y[s];
+                    ret = bdf_ls_setup<MT, LinT>(off, yv, wg, jbad, lane) ? cv::CONV_RECVR : 0;
+                    if (ret) break;
+                }
+                double delp = 0.0;
+                ret = 0;
+                bool converged = false;
+#pragma unroll 1
+                for (int m = 0;; ++m) {
+                    S.cnt[C_NNI]++;
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) delta[s] = -delta[s];
+                    bdf_solve<MT, LinT>(off, delta, wg, lane);
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) acor[s] += delta[s];
+                    const double del = wrms_v<NS>(delta, ewt, N);
+                    if (m > 0) S.crate = fmax(cv::CRDOWN * S.crate, del / delp);
+                    const double dcon = del * fmin(1.0, S.crate) / S.tq[4];
+                    if (dcon <= 1.0) {
+                        S.acnrm = (m == 0) ? del : wrms_v<NS>(acor, ewt, N);
+                        S.jcur = 0;
+                        converged = true;
+                        break;
+                    }
+                    if (m >= 1 && del > cv::RDIV * delp) { ret = cv::CONV_RECVR; break; }
+                    delp = del;
+                    if (m + 1 >= cv::NLS_MAXCOR) { ret = cv::CONV_RECVR; break; }
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + 32 * s] + acor[s];
+                    bdf_rhs<MT, LinT>(off, y, ftemp, lane);
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + 32 * s] + acor[s]);
+                }
+                if (converged) { ret = 0; break; }
+                if (ret == cv::CONV_RECVR && !S.jcur) {
+                    call_setup = 1;
+                    jbad = 1;
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) acor[s] = 0.0;
+                    continue;
+                }
+                break;
+            }
+            nflag = ret;
+            // ---- cvHandleNFlag
+            if (nflag != 0) {
+                S.cnt[C_NCFN]++;
+                S.tn = saved_t;
+                bdf_pascal<MT, LinT>(off, lane, false);
+                ncf++;
+                S.etamax = 1.0;
+                if (ncf == cv::MXNCF) { kflag = cv::CV_CONV_FAILURE; break; }
+                S.eta = cv::ETACF;
+                nflag = cv::PREV_CONV_FAIL;
+                bdf_rescale<MT, LinT>(off, lane);
+                continue;
+            }
+            // ---- cvDoErrorTest
+            dsm = S.acnrm * S.tq[2];
+            if (dsm > 1.0) {
+                nef++;
+                nflag = cv::PREV_ERR_FAIL;
+                const int ef = bdf_error_fail<MT, LinT>(off, dsm, saved_t, nef, lane);
+                if (ef == cv::TRY_AGAIN) continue;
+                kflag = ef;
+                break;
+            }
+            // ---- cvCompleteStep
+            S.nst++;
+            S.hu = S.h;
+            {
+                const int q = S.q;
+                for (int i = q; i >= 2; --i) S.tau[i] = S.tau[i - 1];
+                if (q == 1 && S.nst > 1) S.tau[2] = S.tau[1];
+                S.tau[1] = S.h;
+#pragma unroll 1
+                for (int j = 0; j <= q; ++j) {
+                    const double lj = S.l[j];
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) w->zn[j][lane + 32 * s] += lj * acor[s];
+                }
+                S.qwait--;
+                if (S.qwait == 1 && q != S.qmax) {
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + 32 * s] = acor[s];
+                    S.saved_tq5 = S.tq[5];
+                    S.indx_acor = S.qmax;
+                }
+            }
+            {
+                Vec<NS> av, ev;
+#pragma unroll
+                for (int s = 0; s < NS; ++s) { av.v[s] = acor[s]; ev.v[s] = ewt[s]; }
+                bdf_prepare_next_step<MT, LinT>(off, dsm, av, ev, lane);
+            }
+            S.etamax = (S.nst <= cv::SMALL_NST) ? cv::ETAMX2 : cv::ETAMX3;
+            kflag = 0;
+            break;
+        }
+        if (kflag != 0) { done = true; return kflag; }
+        S.nstloc++;
+        if ((S.tn - tout) * S.h >= 0.0) { done = true; return 0; }
     }
+    return 0;
+}
 
-    // ------------------------------------------- state in HBM (step form)
-    // Per-cell record of the one-launch-per-step form: method scalars and
-    // arrays, the Nordsieck history and the Newton-matrix factors (the saved
-    // Jacobian lives in the cell's WarpGlobal).
-    struct Scalars {
-        double l[8], tq[8], tau[8];
-        double tn, h, hprime, hscale, eta, etamax, hu, saved_tq5, gamma, gammap, gamrat, rl1,
-            crate, acnrm, etaq, etaqm1, etaqp1, P;
-        int q, qprime, qwait, L, indx_acor, jcur, convfail, nst, nstlp, nstlj, nstloc;
-        int status, phase, cnt[7];
-    };
-    static constexpr size_t kScalarBytes = (sizeof(Scalars) + 255) & ~size_t(255);
+// ------------------------------------------------- state in HBM (step form)
+// Per-cell record of the one-launch-per-step form: the method state, the
+// Nordsieck history and the Newton-matrix factors (the saved Jacobian lives in
+// the cell's WarpGlobal).
+template <class MT, class LinT>
+struct StepRecord {
+    static constexpr int N = MT::N;
+    static constexpr size_t kStateBytes = (sizeof(BdfState) + 255) & ~size_t(255);
     static constexpr size_t kZnBytes = ((cv::QMAX + 1) * N * sizeof(double) + 255) & ~size_t(255);
-    static constexpr size_t kLuBytes =
-        ((N * MT::LDA + N) * sizeof(LinT) + N * sizeof(int) + 255) & ~size_t(255);
-    static constexpr size_t kRecordBytes = kScalarBytes + kZnBytes + kLuBytes;
-
-    __device__ __forceinline__ void save(unsigned char* rec, int status, int phase, bool lu_dirty_) const {
-        Scalars* S = reinterpret_cast<Scalars*>(rec);
-        if (lane < 8) { S->l[lane] = sm->l[lane]; S->tq[lane] = sm->tq[lane]; S->tau[lane] = sm->tau[lane]; }
-        if (lane == 0) {
-            S->tn = tn; S->h = h; S->hprime = hprime; S->hscale = hscale; S->eta = eta;
-            S->etamax = etamax; S->hu = hu; S->saved_tq5 = saved_tq5; S->gamma = gamma;
-            S->gammap = gammap; S->gamrat = gamrat; S->rl1 = rl1; S->crate = crate; S->acnrm = acnrm;
-            S->etaq = etaq; S->etaqm1 = etaqm1; S->etaqp1 = etaqp1; S->P = P;
-            S->q = q; S->qprime = qprime; S->qwait = qwait; S->L = L; S->indx_acor = indx_acor;
-            S->jcur = jcur; S->convfail = convfail; S->nst = nst; S->nstlp = nstlp; S->nstlj = nstlj;
-            S->nstloc = nstloc; S->status = status; S->phase = phase;
-            S->cnt[0] = cnt.nst; S->cnt[1] = cnt.nfe; S->cnt[2] = cnt.nje; S->cnt[3] = cnt.nsetups;
-            S->cnt[4] = cnt.nni; S->cnt[5] = cnt.ncfn; S->cnt[6] = cnt.netf;
-        }
-        double* Z = reinterpret_cast<double*>(rec + kScalarBytes);
-        for (int j = 0; j <= cv::QMAX; ++j) {
-            const double* z = zn(j);
-#pragma unroll
-            for (int s = 0; s < NS; ++s)
-                if (valid(s)) Z[j * N + lane + 32 * s] = z[32 * s];
-        }
-        if (lu_dirty_) {
-            LinT* Ag = reinterpret_cast<LinT*>(rec + kScalarBytes + kZnBytes);
-            for (int e = lane; e < N * MT::LDA; e += 32) Ag[e] = sm->A[e];
-            for (int e = lane; e < N; e += 32) Ag[N * MT::LDA + e] = sm->dinv[e];
-            int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA + N);
-            for (int e = lane; e < N; e += 32) pg[e] = sm->perm[e];
-        }
-    }
-    __device__ __forceinline__ void load(const unsigned char* rec, int& status, int& phase) {
-        const Scalars* S = reinterpret_cast<const Scalars*>(rec);
-        if (lane < 8) { sm->l[lane] = S->l[lane]; sm->tq[lane] = S->tq[lane]; sm->tau[lane] = S->tau[lane]; }
-        tn = S->tn; h = S->h; hprime = S->hprime; hscale = S->hscale; eta = S->eta;
-        etamax = S->etamax; hu = S->hu; saved_tq5 = S->saved_tq5; gamma = S->gamma;
-        gammap = S->gammap; gamrat = S->gamrat; rl1 = S->rl1; crate = S->crate; acnrm = S->acnrm;
-        etaq = S->etaq; etaqm1 = S->etaqm1; etaqp1 = S->etaqp1; P = S->P;
-        q = S->q; qprime = S->qprime; qwait = S->qwait; L = S->L; indx_acor = S->indx_acor;
-        jcur = S->jcur; convfail = S->convfail; nst = S->nst; nstlp = S->nstlp; nstlj = S->nstlj;
-        nstloc = S->nstloc; status = S->status; phase = S->phase;
-        cnt.nst = S->cnt[0]; cnt.nfe = S->cnt[1]; cnt.nje = S->cnt[2]; cnt.nsetups = S->cnt[3];
-        cnt.nni = S->cnt[4]; cnt.ncfn = S->cnt[5]; cnt.netf = S->cnt[6];
-        const double* Z = reinterpret_cast<const double*>(rec + kScalarBytes);
-        for (int j = 0; j <= cv::QMAX; ++j) {
-            double* z = zn(j);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) z[32 * s] = valid(s) ? Z[j * N + lane + 32 * s] : 0.0;
-        }
-        const LinT* Ag = reinterpret_cast<const LinT*>(rec + kScalarBytes + kZnBytes);
-        for (int e = lane; e < N * MT::LDA; e += 32) sm->A[e] = Ag[e];
-        for (int e = lane; e < N; e += 32) sm->dinv[e] = Ag[N * MT::LDA + e];
-        const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA + N);
-        for (int e = lane; e < N; e += 32) sm->perm[e] = pg[e];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) acor[s] = tempv[s] = ftemp[s] = y[s] = delta[s] = 0.0;
-        __syncwarp();
-    }
+    static constexpr size_t kLuBytes = ((N * MT::LDA + N) * sizeof(LinT) + N * sizeof(int) + 255) & ~size_t(255);
+    static constexpr size_t kBytes = kStateBytes + 8 + kZnBytes + kLuBytes;   // + phase word
+    static constexpr size_t kPhaseOff = kStateBytes;
 };
+
+template <class MT, class LinT>
+__device__ __noinline__ void bdf_save(unsigned off, unsigned char* rec, int phase, int lane) {
+    using R = StepRecord<MT, LinT>;
+    constexpr int N = MT::N;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    const int* src = reinterpret_cast<const int*>(&w->st);
+    int* dst = reinterpret_cast<int*>(rec);
+#pragma unroll 1
+    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
+    if (lane == 0) *reinterpret_cast<int*>(rec + R::kPhaseOff) = phase;
+    double* Z = reinterpret_cast<double*>(rec + R::kStateBytes + 8);
+    for (int j = 0; j <= cv::QMAX; ++j)
+#pragma unroll
+        for (int s = 0; s < MT::NS; ++s)
+            if (valid_el<MT::NS>(lane, s, N)) Z[j * N + lane + 32 * s] = w->zn[j][lane + 32 * s];
+    if (w->st.lu_dirty) {
+        LinT* Ag = reinterpret_cast<LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
+#pragma unroll 1
+        for (int e = lane; e < N * MT::LDA; e += 32) Ag[e] = w->A[e];
+        for (int e = lane; e < N; e += 32) Ag[N * MT::LDA + e] = w->dinv[e];
+        int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA + N);
+        for (int e = lane; e < N; e += 32) pg[e] = w->perm[e];
+    }
+    __syncwarp();
+}
+
+template <class MT, class LinT>
+__device__ __noinline__ void bdf_load(unsigned off, const unsigned char* rec, int lane) {
+    using R = StepRecord<MT, LinT>;
+    constexpr int N = MT::N;
+    WarpSmem<MT, LinT>* w = wsm<MT, LinT>(off);
+    const int* src = reinterpret_cast<const int*>(rec);
+    int* dst = reinterpret_cast<int*>(&w->st);
+#pragma unroll 1
+    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
+    const double* Z = reinterpret_cast<const double*>(rec + R::kStateBytes + 8);
+    for (int j = 0; j <= cv::QMAX; ++j)
+#pragma unroll
+        for (int s = 0; s < MT::NS; ++s)
+            w->zn[j][lane + 32 * s] = valid_el<MT::NS>(lane, s, N) ? Z[j * N + lane + 32 * s] : 0.0;
+    const LinT* Ag = reinterpret_cast<const LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
+#pragma unroll 1
+    for (int e = lane; e < N * MT::LDA; e += 32) w->A[e] = Ag[e];
+    for (int e = lane; e < N; e += 32) w->dinv[e] = Ag[N * MT::LDA + e];
+    const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA + N);
+    for (int e = lane; e < N; e += 32) w->perm[e] = pg[e];
+    __syncwarp();
+}
 
 }  // namespace b200

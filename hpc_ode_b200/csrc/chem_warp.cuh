@@ -57,6 +57,21 @@ struct Vec {
     double v[NS];
 };
 
+// The kernels' dynamic shared memory.  Out-of-line phases receive byte offsets
+// into it (not pointers) and rebuild typed pointers here, so every access
+// compiles to a shared-memory instruction instead of a generic one.
+__device__ __forceinline__ unsigned char* dyn_smem() {
+    extern __shared__ __align__(16) unsigned char b200_dyn_smem[];
+    return b200_dyn_smem;
+}
+__device__ __forceinline__ unsigned smem_off(const void* p) {
+    return (unsigned)((const unsigned char*)p - dyn_smem());
+}
+template <class T>
+__device__ __forceinline__ T* smem_at(unsigned off) {
+    return reinterpret_cast<T*>(dyn_smem() + off);
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -165,8 +180,69 @@ struct RxnOut {
     double phi, thd, dphi_dthd, dphi_dT, dlnkf_dT;
 };
 
+// Falloff blending of one reaction (Lindemann or Troe): sets phi and, with
+// Deriv, its derivatives.  Out of line: one reaction group of the mechanism
+// uses it, and keeping it out of the reaction loop keeps that loop small.
+struct FallOut {
+    double phi, dphi_dthd, dphi_dT;
+};
+
 template <bool Deriv>
-__device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int s, const CellThermo& c,
+__device__ __noinline__ FallOut falloff(int mech_id, int s, int fl, double T, double logT, double invT,
+                                        double kf, double thd) {
+    const DevMech& M = c_mech[mech_id];
+    const int type = fl & kFlagTypeMask;
+    struct { double T, logT, invT; } c = {T, logT, invT};
+    FallOut o;
+    o.dphi_dthd = 0.0;
+    o.dphi_dT = 0.0;
+    const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
+    const double b0 = __ldg(M.b0 + s), EaR0 = __ldg(M.EaR0 + s);
+    const double k0 = (fl & kFlagConstK0) ? __ldg(M.A0const + s)
+                                          : exp(__ldg(M.logA0 + s) + b0 * c.logT - EaR0 * c.invT);
+    const double Pr = k0 * thd / kf;
+    double F = 1.0, dl_dx = 0.0, dl_dT = 0.0;
+    if (type == 3) {
+        const double a = __ldg(M.troe_a + s), iT3 = __ldg(M.troe_iT3 + s), iT1 = __ldg(M.troe_iT1 + s);
+        const double e3 = exp(-c.T * iT3), e1 = exp(-c.T * iT1);
+        double Fcent = (1.0 - a) * e3 + a * e1;
+        double dFcent = 0.0;
+        if (Deriv) dFcent = -(1.0 - a) * iT3 * e3 - a * iT1 * e1;
+        if (fl & kFlagT2) {
+            const double T2 = __ldg(M.troe_T2 + s);
+            const double e2 = exp(-T2 * c.invT);
+            Fcent += e2;
+            if (Deriv) dFcent += T2 * c.invT * c.invT * e2;
+        }
+        const double Fc = log10(fmax(Fcent, 1.0e-300));
+        const double x = log10(fmax(Pr, 1.0e-300));
+        const double A = x - 0.67 * Fc - 0.4;
+        const double B = 0.806 - 1.1762 * Fc - 0.14 * x;
+        const double u = A / B;
+        const double den = 1.0 + u * u;
+        F = exp10(Fc / den);
+        if (Deriv) {
+            const double du_dx = (B + 0.14 * A) / (B * B);
+            const double du_dFc = (-0.67 * B + 1.1762 * A) / (B * B);
+            dl_dx = (Pr > 1.0e-300) ? -Fc * 2.0 * u * du_dx / (den * den) : 0.0;
+            const double dl_dFc = 1.0 / den - Fc * 2.0 * u * du_dFc / (den * den);
+            const double dFc_dT = (Fcent > 1.0e-300) ? dFcent / (Fcent * 2.302585092994046) : 0.0;
+            dl_dT = dl_dFc * dFc_dT;
+        }
+    }
+    const double blend = Pr / (1.0 + Pr);
+    o.phi = F * blend;
+    if (Deriv) {
+        const double dphi_dPr = F / ((1.0 + Pr) * (1.0 + Pr)) + F / (1.0 + Pr) * dl_dx;
+        o.dphi_dthd = dphi_dPr * (k0 / kf);
+        const double dlnPr_dT = (b0 + EaR0 * c.invT) * c.invT - (b + EaR * c.invT) * c.invT;
+        o.dphi_dT = dphi_dPr * Pr * dlnPr_dT + blend * F * 2.302585092994046 * dl_dT;
+    }
+    return o;
+}
+
+template <bool Deriv>
+__device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int mech_id, int s, const CellThermo& c,
                                            const double* C, const double* G) {
     RxnOut o;
     o.q = 0.0; o.kf = 0.0; o.kr = 0.0; o.Rf = 0.0; o.Rr = 0.0; o.phi = 1.0; o.thd = 0.0;
@@ -198,6 +274,7 @@ __device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int s, const CellTh
         } else {
             thd = c.m;
             const int off = __ldg(M.tb_off + s), len = __ldg(M.tb_len + s);
+#pragma unroll 1
             for (int t = 0; t < len; ++t) thd += __ldg(M.tb_alpha + off + t) * C[__ldg(M.tb_sp + off + t)];
         }
         o.thd = thd;
@@ -205,47 +282,10 @@ __device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int s, const CellTh
             o.phi = thd;
             o.dphi_dthd = 1.0;
         } else {
-            const double b0 = __ldg(M.b0 + s), EaR0 = __ldg(M.EaR0 + s);
-            const double k0 = (fl & kFlagConstK0) ? __ldg(M.A0const + s)
-                                                  : exp(__ldg(M.logA0 + s) + b0 * c.logT - EaR0 * c.invT);
-            const double Pr = k0 * thd / kf;
-            double F = 1.0, dl_dx = 0.0, dl_dT = 0.0;
-            if (type == 3) {
-                const double a = __ldg(M.troe_a + s), iT3 = __ldg(M.troe_iT3 + s), iT1 = __ldg(M.troe_iT1 + s);
-                const double e3 = exp(-c.T * iT3), e1 = exp(-c.T * iT1);
-                double Fcent = (1.0 - a) * e3 + a * e1;
-                double dFcent = 0.0;
-                if (Deriv) dFcent = -(1.0 - a) * iT3 * e3 - a * iT1 * e1;
-                if (fl & kFlagT2) {
-                    const double T2 = __ldg(M.troe_T2 + s);
-                    const double e2 = exp(-T2 * c.invT);
-                    Fcent += e2;
-                    if (Deriv) dFcent += T2 * c.invT * c.invT * e2;
-                }
-                const double Fc = log10(fmax(Fcent, 1.0e-300));
-                const double x = log10(fmax(Pr, 1.0e-300));
-                const double A = x - 0.67 * Fc - 0.4;
-                const double B = 0.806 - 1.1762 * Fc - 0.14 * x;
-                const double u = A / B;
-                const double den = 1.0 + u * u;
-                F = exp10(Fc / den);
-                if (Deriv) {
-                    const double du_dx = (B + 0.14 * A) / (B * B);
-                    const double du_dFc = (-0.67 * B + 1.1762 * A) / (B * B);
-                    dl_dx = (Pr > 1.0e-300) ? -Fc * 2.0 * u * du_dx / (den * den) : 0.0;
-                    const double dl_dFc = 1.0 / den - Fc * 2.0 * u * du_dFc / (den * den);
-                    const double dFc_dT = (Fcent > 1.0e-300) ? dFcent / (Fcent * 2.302585092994046) : 0.0;
-                    dl_dT = dl_dFc * dFc_dT;
-                }
-            }
-            const double blend = Pr / (1.0 + Pr);
-            o.phi = F * blend;
-            if (Deriv) {
-                const double dphi_dPr = F / ((1.0 + Pr) * (1.0 + Pr)) + F / (1.0 + Pr) * dl_dx;
-                o.dphi_dthd = dphi_dPr * (k0 / kf);
-                const double dlnPr_dT = (b0 + EaR0 * c.invT) * c.invT - (b + EaR * c.invT) * c.invT;
-                o.dphi_dT = dphi_dPr * Pr * dlnPr_dT + blend * F * 2.302585092994046 * dl_dT;
-            }
+            const FallOut f = falloff<Deriv>(mech_id, s, fl, c.T, c.logT, c.invT, kf, thd);
+            o.phi = f.phi;
+            o.dphi_dthd = f.dphi_dthd;
+            o.dphi_dT = f.dphi_dT;
         }
     }
     o.q = (o.Rf - o.Rr) * o.phi;
@@ -264,10 +304,9 @@ __device__ __forceinline__ void gather(const DevMech& M, const double* src, Chem
     for (int e = 0; e < gmax; ++e) {
         const int w = __ldg(gw + 32 * e);
         acc += (double)(((w >> 11) & 31) - 16) * src[w & 2047];
-        if (w & (1 << 16)) {
-            sm->part[w >> 17] = acc;
-            acc = 0.0;
-        }
+        const bool last = (w >> 16) & 1;
+        if (last) sm->part[w >> 17] = acc;
+        acc = last ? 0.0 : acc;
     }
     __syncwarp();
 #pragma unroll
@@ -285,9 +324,10 @@ __device__ __forceinline__ void gather(const DevMech& M, const double* src, Chem
 
 // f = dy/dt for the warp's cell.  y, f: lane elements in internal order.
 template <class MT>
-__device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, ChemSmem<MT>* sm, int lane) {
+__device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, unsigned chem_off, int lane) {
     constexpr int N = MT::N;
     const DevMech& M = mech<MT>();
+    ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
     double y[MT::NS];
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) y[s] = yv.v[s];
@@ -296,7 +336,7 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, Che
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        sm->q[s] = rxn_eval<false>(M, s, c, sm->C, sm->G).q;
+        sm->q[s] = rxn_eval<false>(M, MT::ID, s, c, sm->C, sm->G).q;
     }
     __syncwarp();
     double om[MT::NS];
@@ -331,21 +371,24 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, Che
 // d q / d C_j is scattered into the species-space rows with shared-memory
 // atomics (one warp per cell, so the accumulation never leaves the warp).
 template <class MT, class LinT>
-__device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, LinT* A, ChemSmem<MT>* sm,
+__device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A_off, unsigned chem_off,
                                       JacScratch<MT>* js, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
     const DevMech& M = mech<MT>();
+    LinT* A = smem_at<LinT>(A_off);
+    ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
     double y[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) y[s] = yv.v[s];
     double Yk[NS], cpR[NS], hRT[NS], dcpR[NS];
+#pragma unroll 2
     for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
     const int ns = M.nslot;
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        const RxnOut o = rxn_eval<true>(M, s, c, sm->C, sm->G);
+        const RxnOut o = rxn_eval<true>(M, MT::ID, s, c, sm->C, sm->G);
         const int fl = __ldg(M.flags + s);
         double dqdT = 0.0, sr = 0.0, thd_term = 0.0;
         double dRf[3] = {0.0, 0.0, 0.0}, dRr[3] = {0.0, 0.0, 0.0};
@@ -404,9 +447,11 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, LinT* A, C
                 const double tt = nu * thd_term;
                 if (cat >= 0) {
                     // [M] = m - sum_{k != cat} C_k: d[M]/dC_j = -1 for j != cat
+#pragma unroll 1
                     for (int j = 0; j < N; ++j)
                         if (j != cat) atomicAdd(row + j, (LinT)(-tt));
                 } else {
+#pragma unroll 1
                     for (int t = 0; t < len; ++t)
                         atomicAdd(row + __ldg(M.tb_sp + off + t), (LinT)(tt * __ldg(M.tb_alpha + off + t)));
                 }
@@ -459,6 +504,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, LinT* A, C
         trow[s] = 0.0;
         if (j < N - 1) {
             double S1 = 0.0;
+#pragma unroll 4
             for (int k = 0; k < N; ++k) S1 += spw[k] * (double)A[k * LDA + j];
             const double Wj = __ldg(M.mw + j);
             const double dj = 1.0 / Wj - 1.0 / WN;
@@ -475,6 +521,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, LinT* A, C
             const double Wk = __ldg(M.mw + k);
             const double cN = (double)row[N - 1] / WN;
             const double X = spw[2 * N + k];
+#pragma unroll 4
             for (int j = 0; j < N - 1; ++j) {
                 const double iWj = __ldg(M.inv_mw + j);
                 row[j] = (LinT)(Wk * ((double)row[j] * iWj - cN + X * (iWj - 1.0 / WN)));

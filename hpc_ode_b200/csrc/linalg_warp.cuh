@@ -28,8 +28,11 @@ __device__ __forceinline__ T absT(T v) { return v < T(0) ? -v : v; }
 // composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
 // Returns 0, or k+1 if U_kk == 0 (singular).  All 32 lanes call it.
 template <class MT, class LinT>
-__device__ __noinline__ int warp_lu(LinT* A, int* perm, LinT* dinv, int lane) {
+__device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA;
+    LinT* A = smem_at<LinT>(A_off);
+    int* perm = smem_at<int>(perm_off);
+    LinT* dinv = smem_at<LinT>(dinv_off);
     int sing = 0;
     int pv = lane;   // lane i tracks perm[i] for i = lane, lane + 32
     int pv2 = lane + 32;
@@ -50,6 +53,7 @@ __device__ __noinline__ int warp_lu(LinT* A, int* perm, LinT* dinv, int lane) {
         }
         if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
         if (bi != k) {
+#pragma unroll 1
             for (int j = lane; j < N; j += 32) {
                 const LinT t = A[k * LDA + j];
                 A[k * LDA + j] = A[bi * LDA + j];
@@ -85,9 +89,12 @@ __device__ __noinline__ int warp_lu(LinT* A, int* perm, LinT* dinv, int lane) {
 // Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + 32 s) in,
 // solution out.  Arithmetic in LinT.
 template <class MT, class LinT>
-__device__ __noinline__ Vec<MT::NS> warp_lu_solve(const LinT* A, const int* perm, const LinT* dinv,
+__device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_off, unsigned dinv_off,
                                                   const Vec<MT::NS> bv, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    const LinT* A = smem_at<LinT>(A_off);
+    const int* perm = smem_at<int>(perm_off);
+    const LinT* dinv = smem_at<LinT>(dinv_off);
     const double (&b)[NS] = bv.v;
     Vec<NS> out;
     LinT x[NS];
@@ -104,10 +111,12 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(const LinT* A, const int* perm
         }
         x[s] = (i < N) ? (LinT)v : LinT(0);
     }
-    // forward: unit lower
-#pragma unroll
+    // forward: unit lower (rolled: this runs every Newton iteration and must
+    // stay small in the instruction cache)
+#pragma unroll 1
     for (int k = 0; k < N - 1; ++k) {
-        const LinT xk = __shfl_sync(kFull, x[k >> 5], k & 31);
+        const LinT src = (NS == 1 || k < 32) ? x[0] : x[NS - 1];
+        const LinT xk = __shfl_sync(kFull, src, k & 31);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + 32 * s;
@@ -115,10 +124,14 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(const LinT* A, const int* perm
         }
     }
     // backward: upper
-#pragma unroll
+#pragma unroll 1
     for (int k = N - 1; k >= 0; --k) {
-        const LinT xk = __shfl_sync(kFull, x[k >> 5], k & 31) * dinv[k];
-        if (lane == (k & 31)) x[k >> 5] = xk;
+        const LinT src = (NS == 1 || k < 32) ? x[0] : x[NS - 1];
+        const LinT xk = __shfl_sync(kFull, src, k & 31) * dinv[k];
+        if (lane == (k & 31)) {
+            if (NS == 1 || k < 32) x[0] = xk;
+            else x[NS - 1] = xk;
+        }
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + 32 * s;
