@@ -759,3 +759,158 @@ b200ode_status b200ode_fp64_peak(int32_t device, double* gflops) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------- no-allocation entry point
+// b200ode_integrate_device_noalloc runs the persistent BDF kernel with all of
+// its device scratch in one file-scope array instead of the handle's cudaMalloc'd
+// buffers.  It serves callers that must not allocate device memory while they
+// integrate: a flow solver whose own pool has taken the whole device at start-up,
+// or one that cannot accept the device-wide synchronization of cudaFree (which
+// b200ode_integrate_device issues when a larger launch outgrows the handle's
+// scratch) in the middle of its time step.
+//
+// Layout of the array: bytes [0, 256) are the control block (work-queue head,
+// 8 call totals, 5 phase-cycle totals), which every call clears before its
+// launch; from byte 256 on, one WarpGlobal (saved Newton Jacobian and Jacobian
+// rate scratch) per resident warp, which the kernel writes before it reads, so
+// the previous call's contents there do no harm.  The array exists once per
+// device that loads this library and stays reserved until the process exits.
+// Every call on a device uses the same array: calls that overlap on the GPU
+// (different streams, handles or host threads without ordering) race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[B200ODE_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr size_t kNoAllocCtlBytes = 256;
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device`, which must be current.  The
+// host-side name g_noalloc_scratch is only a handle for the runtime; the address
+// is looked up once per device (the first call there) and kept.
+b200ode_status noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices)
+        return fail(B200ODE_ERR_INVALID, "b200ode_integrate_device_noalloc: device ordinal " +
+                                             std::to_string(device) + " out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(B200ODE_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") +
+                                              cudaGetErrorString(e));
+        g_noalloc_ptr[device] = static_cast<unsigned char*>(ptr);
+    }
+    *out = g_noalloc_ptr[device];
+    return B200ODE_OK;
+}
+
+// Makes `device` current for the lifetime of the guard, then restores the
+// caller's device.
+struct NoAllocDeviceGuard {
+    int prev = -1;
+    cudaError_t enter(int device) {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) { prev = -1; return e; }
+        if (prev == device) { prev = -1; return cudaSuccess; }
+        return cudaSetDevice(device);
+    }
+    ~NoAllocDeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+// Same launch shape as the persistent branch of launch_bdf (so both entry points
+// run identical grids), with queue, totals and per-warp scratch in the array.
+template <class MT, class LinT>
+b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* scratch, cudaStream_t st,
+                                  int* launches) {
+    using WG = WarpGlobal<MT, LinT>;
+    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+    auto kern = k_bdf<MT, LinT, 1>;
+    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
+    CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int bps = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, wpb * 32, smem));
+    if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
+    if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
+    const size_t n = (size_t)p.ncells;
+    long long blocks = (long long)bps * h->num_sms;
+    blocks = std::max(1LL, std::min(blocks, (long long)((n + wpb - 1) / wpb)));
+    const size_t need = kNoAllocCtlBytes + (size_t)blocks * wpb * sizeof(WG);
+    if (need > (size_t)B200ODE_NOALLOC_SCRATCH_BYTES)
+        return fail(B200ODE_ERR_INVALID,
+                    "b200ode_integrate_device_noalloc: this launch needs " + std::to_string(need) +
+                        " bytes of scratch (" + std::to_string(blocks) + " blocks x " + std::to_string(wpb) +
+                        " warps x " + std::to_string(sizeof(WG)) + " bytes + 256) but the static scratch holds " +
+                        std::to_string((size_t)B200ODE_NOALLOC_SCRATCH_BYTES) +
+                        " bytes; lower options.blocks_per_sm or options.warps_per_block");
+    h->last_blocks_per_sm = bps;
+    auto* ctl = reinterpret_cast<unsigned long long*>(scratch);
+    CUDA_TRY(cudaMemsetAsync(ctl, 0, kNoAllocCtlBytes, st));
+    p.queue = ctl;
+    p.totals = ctl + 1;
+    p.done_count = ctl + 9;
+    p.prof = h->opt.profile_phases ? ctl + 10 : nullptr;
+    p.wglobal = scratch + kNoAllocCtlBytes;
+    p.records = nullptr;
+    p.steps = 0x7fffffff;
+    kern<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+    CUDA_TRY(cudaGetLastError());
+    *launches += 1;
+    return B200ODE_OK;
+}
+
+}  // namespace
+
+extern "C" b200ode_status b200ode_integrate_device_noalloc(b200ode_handle* h, int64_t n, const double* dP,
+                                                           double Ps, double* dT, double* dY, double t0,
+                                                           double t1, int32_t* dstat, b200ode_stats* stats,
+                                                           void* stream) {
+    b200ode_status rc = check_args(h, n, t0, t1);
+    if (rc != B200ODE_OK) return rc;
+    int32_t* dcnt[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    if (stats) {
+        int32_t* keep[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+        std::memset(stats, 0, sizeof(*stats));
+        stats->nst = keep[0]; stats->nfe = keep[1]; stats->nje = keep[2]; stats->nsetups = keep[3];
+        stats->nni = keep[4]; stats->ncfn = keep[5]; stats->netf = keep[6];
+        for (int i = 0; i < 7; ++i) dcnt[i] = keep[i];
+    }
+    if (n == 0) return B200ODE_OK;
+    if (!dT || !dY) return fail(B200ODE_ERR_INVALID, "null T or Y");
+    if (!dP && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
+    NoAllocDeviceGuard guard;
+    CUDA_TRY(guard.enter(h->device));
+    unsigned char* scratch = nullptr;
+    rc = noalloc_scratch(h->device, &scratch);
+    if (rc != B200ODE_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    KParams p;
+    fill_params(h, p, n, dP, Ps, dT, dY, dstat, dcnt, t0, t1);
+    int launches = 0;
+    CUDA_TRY(cudaEventRecord(h->ev[1], st));
+    const bool fp64 = h->opt.precision == B200ODE_FP64;
+    if (h->mech == MECH_GRI30)
+        rc = fp64 ? launch_bdf_noalloc<GriT, double>(h, p, scratch, st, &launches)
+                  : launch_bdf_noalloc<GriT, float>(h, p, scratch, st, &launches);
+    else
+        rc = fp64 ? launch_bdf_noalloc<H2T, double>(h, p, scratch, st, &launches)
+                  : launch_bdf_noalloc<H2T, float>(h, p, scratch, st, &launches);
+    if (rc != B200ODE_OK) return rc;
+    CUDA_TRY(cudaEventRecord(h->ev[2], st));
+    if (stats) {
+        unsigned long long t[15];
+        CUDA_TRY(cudaMemcpyAsync(t, scratch + sizeof(unsigned long long), sizeof(t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < 5; ++i) stats->phase_cycles[i] = h->opt.profile_phases ? (int64_t)t[9 + i] : 0;
+        stats->total_nst = (int64_t)t[0]; stats->total_nfe = (int64_t)t[1]; stats->total_nje = (int64_t)t[2];
+        stats->total_nsetups = (int64_t)t[3]; stats->total_nni = (int64_t)t[4]; stats->total_ncfn = (int64_t)t[5];
+        stats->total_netf = (int64_t)t[6]; stats->n_failed = (int64_t)t[7];
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+        stats->kernel_ms = ms;
+        stats->gpu_launches = launches;
+    }
+    return B200ODE_OK;
+}

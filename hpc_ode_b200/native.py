@@ -24,7 +24,8 @@ CELL_STATUS = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC",
 
 # Every symbol include/b200ode.h declares.
 EXPORTED = ["b200ode_default_options", "b200ode_create", "b200ode_destroy", "b200ode_num_species",
-            "b200ode_integrate", "b200ode_integrate_device", "b200ode_eval_rhs",
+            "b200ode_integrate", "b200ode_integrate_device", "b200ode_integrate_device_noalloc",
+            "b200ode_eval_rhs",
             "b200ode_eval_jacobian", "b200ode_fp64_peak",
             "b200ode_last_error", "b200ode_version"]
 
@@ -88,6 +89,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
                                              C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                              C.c_void_p, C.POINTER(Stats), C.c_void_p]
     lib.b200ode_integrate_device.restype = C.c_int
+    lib.b200ode_integrate_device_noalloc.argtypes = lib.b200ode_integrate_device.argtypes
+    lib.b200ode_integrate_device_noalloc.restype = C.c_int
     lib.b200ode_eval_rhs.argtypes = [C.c_void_p, C.c_int64, _dp, C.c_double, _dp, _dp, _dp, _dp]
     lib.b200ode_eval_rhs.restype = C.c_int
     lib.b200ode_eval_jacobian.argtypes = [C.c_void_p, C.c_int64, _dp, C.c_double, _dp, _dp, _dp]
@@ -198,6 +201,18 @@ class Solver:
         """Device-pointer integration (pointers as ints, e.g. torch tensor.data_ptr())."""
         st = Stats() if want_stats else None
         _check(self.lib.b200ode_integrate_device(
+            self.h, n, C.c_void_p(dP or None), float(P_scalar), C.c_void_p(dT), C.c_void_p(dY),
+            float(t0), float(t1), C.c_void_p(dstatus or None),
+            C.byref(st) if st is not None else None, C.c_void_p(stream or None)))
+        self.last_stats = st
+        return stats_dict(st) if st is not None else None
+
+    def integrate_device_noalloc(self, n: int, dP: int, P_scalar: float, dT: int, dY: int, t1: float,
+                                 t0: float = 0.0, dstatus: int = 0, stream: int = 0, want_stats=True):
+        """As integrate_device, through the entry point that allocates no device
+        memory (its scratch is one static array per device, shared by every call)."""
+        st = Stats() if want_stats else None
+        _check(self.lib.b200ode_integrate_device_noalloc(
             self.h, n, C.c_void_p(dP or None), float(P_scalar), C.c_void_p(dT), C.c_void_p(dY),
             float(t0), float(t1), C.c_void_p(dstatus or None),
             C.byref(st) if st is not None else None, C.c_void_p(stream or None)))

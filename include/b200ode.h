@@ -125,6 +125,44 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, cons
                                         double t1, int32_t* d_cell_status, b200ode_stats* stats,
                                         void* stream);
 
+/* Size of the static device scratch of b200ode_integrate_device_noalloc. */
+#define B200ODE_NOALLOC_SCRATCH_BYTES (24u << 20)
+
+/* b200ode_integrate_device without any device allocation.  No counterpart in
+ * the reference.
+ *
+ * For callers that must not allocate device memory while they integrate: a flow
+ * solver whose memory pool has taken the whole GPU at start-up, or one that
+ * cannot accept, in the middle of its time step, the device-wide
+ * synchronization of cudaFree (b200ode_integrate_device frees and re-allocates
+ * its per-handle scratch when a larger launch outgrows it).  Arguments, results
+ * and per-cell semantics are those of b200ode_integrate_device; the caller
+ * passes every input and output buffer.  This call makes no cudaMalloc, cudaFree
+ * or other allocating call: the work-queue head, the call totals and the
+ * per-warp Newton scratch live in one static device array of
+ * B200ODE_NOALLOC_SCRATCH_BYTES (24 MiB), which every GPU that loads this
+ * library keeps until the process exits.
+ *
+ *  - Always runs the persistent kernel (options.persistent and use_graph are
+ *    not used).  A launch needs 256 bytes + resident warps x per-warp scratch
+ *    (16.9 KB for GRI-Mech 3.0 in mixed precision, 28.1 KB in FP64); one that
+ *    needs more than the array is refused with B200ODE_ERR_INVALID and the
+ *    numbers in b200ode_last_error().  On a 148-SM B200 every launch shape the
+ *    options allow fits; the number of cells is not limited.
+ *  - The first call on a device looks up the array's device address there (and,
+ *    with lazy module loading, is when the driver loads this library's kernels
+ *    onto that device).  Make that first call before any stream capture.
+ *  - Every call on a device shares the one array, which keeps the previous
+ *    call's contents; each call clears the part that must start at zero.  Calls
+ *    that overlap on the GPU (different streams, handles or host threads without
+ *    ordering between them) race on the array and give wrong results.
+ *  - Asynchronous unless stats is non-NULL (then it synchronizes the stream to
+ *    fill the totals). */
+b200ode_status b200ode_integrate_device_noalloc(b200ode_handle* h, int64_t n_cells, const double* d_P,
+                                                double P_scalar, double* d_T, double* d_Y, double t0,
+                                                double t1, int32_t* d_cell_status, b200ode_stats* stats,
+                                                void* stream);
+
 /* Chemistry source terms alone, one GPU warp per cell (host buffers).
  * Counterparts of the reference's batched pyJac kernels dydt_cvode_GPU /
  * kernel_dydt (src/Integrators/Drivers/CVodeGPUDriver.cu:28-65, 299-313) and of
