@@ -36,6 +36,10 @@ sys.path.insert(0, ROOT)
 from hpc_ode_b200 import workloads as W  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20
+# DRAM bytes per cell of one k_bdf launch, from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum, 8,192-cell GRI capture, mixed precision): the traffic
+# is the compulsory T/P/Y in + T/Y/status out, so it scales with the cell count.
+NCU_DRAM_BYTES_PER_CELL = {"gri30": 861.0}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -169,7 +173,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--form", default="persistent", choices=["persistent", "step"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=1024)
+    ap.add_argument("--cpu-sample", type=int, default=8192,
+                    help="cells of the workload the CPU baseline integrates per step (stratified)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -288,8 +293,14 @@ def main():
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     alg_bytes = n * ((nsp + 1) * 8 + 8) + n * ((nsp + 1) * 8 + 4)   # T,Y,P in; T,Y,status out
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    per_cell = NCU_DRAM_BYTES_PER_CELL.get(batch.mech)
+    traffic = per_cell * n if per_cell else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved / hbm_peak, "traffic": None,
+                "frac": achieved / hbm_peak, "traffic": traffic,
+                "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 8,192-cell "
+                                   "k_bdf launch (profiles/k_bdf_gri8k_mixed_full.txt), scaled by cells"
+                                   if per_cell else None),
+                "alg_bytes": alg_bytes,
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
                 "note": "compute-bound path (FP64 CUDA-core pipe); HBM fraction shown for the "
                         "contract, see fp64 block and profiles/"}
