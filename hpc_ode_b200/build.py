@@ -18,6 +18,8 @@ LIB = os.path.join(PKG, "libb200ode.so")
 HOST_LIB = os.path.join(PKG, "libb200ode_host.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# translation units of libb200ode.so: kernels + integrate ABI, request loop
+CU_SOURCES = ["b200ode.cu", "serve.cu"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
               "--expt-relaxed-constexpr"]
 
@@ -35,7 +37,8 @@ def _sources():
         for f in fs:
             if f.endswith((".cu", ".cuh", ".h", ".hpp", ".cpp")):
                 out.append(os.path.join(d, f))
-    out.append(os.path.join(ROOT, "include", "b200ode.h"))
+    inc = os.path.join(ROOT, "include")
+    out.extend(os.path.join(inc, f) for f in os.listdir(inc))
     return out
 
 
@@ -49,7 +52,7 @@ def _stale(target: str) -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale(LIB):
         cmd = [_nvcc(), *ARCH, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"),
-               "-o", LIB + ".tmp", os.path.join(CSRC, "b200ode.cu")]
+               "-o", LIB + ".tmp", *(os.path.join(CSRC, f) for f in CU_SOURCES)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/b200ode.h"
+#include "b200ode_internal.h"
 #include "bdf_warp.cuh"
 #include "mech/gri30_mech.h"
 #include "mech/h2o2_mech.h"
@@ -264,29 +265,7 @@ __global__ void k_fp64_peak(double* out, int iters) {
 }
 
 // ------------------------------------------------------------------ handle
-struct b200ode_handle {
-    int mech = -1;
-    HostMech hm;
-    unsigned char* d_blob = nullptr;
-    DevMech dm;
-    b200ode_options opt;
-    int device = 0, num_sms = 0;
-    size_t cap = 0;   // cells
-    double* d_T = nullptr;
-    double* d_Y = nullptr;
-    double* d_P = nullptr;
-    int32_t* d_status = nullptr;
-    int32_t* d_cnt = nullptr;
-    unsigned long long* d_ctl = nullptr;   // [0] queue, [1..8] totals
-    void* d_wg = nullptr;                    // WarpGlobal scratch (saved Jacobians, ...)
-    size_t wg_bytes = 0;
-    unsigned char* d_rec = nullptr;          // step-form per-cell records
-    size_t rec_bytes = 0;
-    unsigned long long* h_done = nullptr;    // pinned host copy of the done counter
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    int last_blocks_per_sm = 0;
-};
+// struct b200ode_handle: b200ode_internal.h
 
 namespace {
 
@@ -390,6 +369,36 @@ b200ode_status run(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches
     return fp64 ? launch_bdf<H2T, double>(h, p, st, launches) : launch_bdf<H2T, float>(h, p, st, launches);
 }
 
+// Calls f(MT{}, LinT{}) with the handle's mechanism and Newton-matrix precision.
+template <class F>
+b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
+    const bool fp64 = h->opt.precision == B200ODE_FP64;
+    if (h->mech == MECH_GRI30) return fp64 ? f(GriT{}, double{}) : f(GriT{}, float{});
+    return fp64 ? f(H2T{}, double{}) : f(H2T{}, float{});
+}
+
+// Launch shape of the persistent form: the same choice launch_bdf makes.
+template <class MT, class LinT>
+b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KParams), long long* blocks,
+                                int* wpb_out, size_t* smem_out) {
+    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+    auto k = k_bdf<MT, LinT, 1>;
+    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) k = k_bdf<MT, LinT, 3>;
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int bps = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, wpb * 32, smem));
+    if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
+    if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
+    long long b = (long long)bps * h->num_sms;
+    b = std::max(1LL, std::min(b, (n + wpb - 1) / wpb));
+    *kern = k;
+    *blocks = b;
+    *wpb_out = wpb;
+    *smem_out = smem;
+    return B200ODE_OK;
+}
+
 template <class MT, class LinT>
 b200ode_status launch_eval(b200ode_handle* h, KParams& p, double* d_dT, double* d_dY, double* d_jac,
                            cudaStream_t st) {
@@ -469,6 +478,58 @@ b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st)
 
 }  // namespace
 
+// ------------------------------------------------- internal API (b200ode_internal.h)
+namespace b200 {
+
+b200ode_status set_error(b200ode_status st, const std::string& msg) { return fail(st, msg); }
+
+size_t persistent_scratch_bytes(b200ode_handle* h, int64_t n) {
+    size_t bytes = 0;
+    dispatch_mech(h, [&](auto mt, auto lt) {
+        using MT = decltype(mt);
+        using LinT = decltype(lt);
+        void (*k)(KParams) = nullptr;
+        long long blocks = 0;
+        int wpb = 0;
+        size_t smem = 0;
+        b200ode_status rc = persistent_shape<MT, LinT>(h, std::max<long long>(n, 1), &k, &blocks, &wpb, &smem);
+        if (rc == B200ODE_OK) bytes = (size_t)blocks * wpb * sizeof(WarpGlobal<MT, LinT>);
+        return rc;
+    });
+    return bytes;
+}
+
+b200ode_status launch_persistent(b200ode_handle* h, int64_t n, const double* dP, double Ps, double* dT,
+                                 double* dY, int32_t* dstat, double t0, double t1, unsigned long long* ctl,
+                                 void* wg, cudaStream_t st) {
+    if (n <= 0) return B200ODE_OK;
+    KParams p;
+    fill_params(h, p, n, dP, Ps, dT, dY, dstat, nullptr, t0, t1);
+    p.queue = ctl;
+    p.totals = ctl + 1;
+    p.done_count = ctl + 9;
+    p.prof = h->opt.profile_phases ? ctl + 10 : nullptr;
+    p.wglobal = wg;
+    p.records = nullptr;
+    p.steps = 0x7fffffff;
+    return dispatch_mech(h, [&](auto mt, auto lt) {
+        using MT = decltype(mt);
+        using LinT = decltype(lt);
+        void (*k)(KParams) = nullptr;
+        long long blocks = 0;
+        int wpb = 0;
+        size_t smem = 0;
+        b200ode_status rc = persistent_shape<MT, LinT>(h, n, &k, &blocks, &wpb, &smem);
+        if (rc != B200ODE_OK) return rc;
+        CUDA_TRY(cudaMemsetAsync(ctl, 0, kCtlWords * sizeof(unsigned long long), st));
+        k<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+        CUDA_TRY(cudaGetLastError());
+        return B200ODE_OK;
+    });
+}
+
+}  // namespace b200
+
 // ------------------------------------------------------------------- C ABI
 extern "C" {
 
@@ -494,6 +555,14 @@ const char* b200ode_last_error(void) { return g_last_error.c_str(); }
 const char* b200ode_version(void) { return "b200ode 0.1 (sm_100a)"; }
 
 int32_t b200ode_num_species(const b200ode_handle* h) { return h ? h->hm.nsp : -1; }
+
+int32_t b200ode_mechanism_species(const char* mech_name) {
+    switch (mech_from_name(mech_name)) {
+        case MECH_GRI30: return MECH_GRI30_NSP;
+        case MECH_H2O2: return MECH_H2O2_NSP;
+        default: return -1;
+    }
+}
 
 b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts, b200ode_handle** out) {
     if (!out) return fail(B200ODE_ERR_INVALID, "null output pointer");

@@ -1,0 +1,90 @@
+// B200BDFIntegrator (b200ode_integrator.hpp): the reference's Integrator on
+// the C ABI of b200ode.h.  The mesh's cell-major rows (temperature[i],
+// species[i][k]) are packed into structure-of-arrays staging (T[i],
+// Y[k * n + i]) for one b200ode_integrate call and unpacked afterwards, which is
+// what CVodeIntegratorGPU::setGPUArrayInitialConditions / saveGPUArrayResults
+// do for its device arrays (src/Integrators/CVodeIntegratorGPU.cpp:128-161).
+#include <cstring>
+#include <sstream>
+#include <stdexcept>
+
+#include "b200ode_integrator.hpp"
+
+B200BDFIntegrator::B200BDFIntegrator() {
+    b200ode_default_options(&opts_);
+    std::memset(&stats_, 0, sizeof(stats_));
+}
+
+B200BDFIntegrator::~B200BDFIntegrator() {
+    if (handle_) b200ode_destroy(handle_);
+    handle_ = nullptr;
+}
+
+void B200BDFIntegrator::setOptions(const b200ode_options& opts) { opts_ = opts; }
+
+void B200BDFIntegrator::init(std::shared_ptr<Context> c, IntegratorConfig config) {
+    Integrator::init(std::move(c), config);
+    // mechanism check before any device work (CVodeIntegrator.cpp:41-48)
+    const int nsp = b200ode_mechanism_species(mechanism.c_str());
+    if (nsp < 0 || systemSize != nsp) {
+        std::stringstream ss;
+        ss << "mechanism size of: " << mechanism << " (" << nsp << ") differs from the mesh size: " << systemSize;
+        logger->error(ss.str());
+        throw std::runtime_error(ss.str());
+    }
+    if (handle_) b200ode_destroy(handle_);
+    handle_ = nullptr;
+    b200ode_options o = opts_;
+    o.reltol = reltol;
+    o.abstol = abstol;
+    const b200ode_status rc = b200ode_create(mechanism.c_str(), &o, &handle_);
+    if (rc != B200ODE_OK) {
+        const std::string msg = std::string("B200BDFIntegrator: ") + b200ode_last_error();
+        logger->error(msg);
+        throw std::runtime_error(msg);
+    }
+    logger->info("B200BDFIntegrator initialized");
+}
+
+void B200BDFIntegrator::integrate(double t0, double t) {
+    Integrator::integrate(t0, t);
+    if (!handle_) throw std::runtime_error("B200BDFIntegrator: integrate() before init()");
+    const int n = mesh->totalSize();
+    const int nsp = systemSize;
+    T_.resize(n);
+    Y_.resize((size_t)n * nsp);
+    status_.assign(n, 0);
+    const double* Tm = mesh->getTemperaturePointer();
+    for (int i = 0; i < n; ++i) {
+        T_[i] = Tm[i];
+        const double* y = mesh->getSpeciesPointer(i);
+        for (int k = 0; k < nsp; ++k) Y_[(size_t)k * n + i] = y[k];
+    }
+    std::memset(&stats_, 0, sizeof(stats_));
+    const b200ode_status rc =
+        b200ode_integrate(handle_, n, nullptr, pressure, T_.data(), Y_.data(), t0, t, status_.data(), &stats_);
+    if (rc != B200ODE_OK) {
+        const std::string msg = std::string("B200BDFIntegrator: ") + b200ode_last_error();
+        logger->error(msg);
+        throw std::runtime_error(msg);
+    }
+    double* Tw = mesh->getTemperaturePointer();
+    for (int i = 0; i < n; ++i) {
+        Tw[i] = T_[i];
+        double* y = mesh->getSpeciesPointer(i);
+        for (int k = 0; k < nsp; ++k) y[k] = Y_[(size_t)k * n + i];
+    }
+    if (stats_.n_failed) {
+        std::stringstream ss;
+        ss << stats_.n_failed << " of " << n << " cells did not reach t (CVODE status kept per cell)";
+        logger->error(ss.str());
+    }
+}
+
+void B200BDFIntegrator::clean() {
+    if (handle_) b200ode_destroy(handle_);
+    handle_ = nullptr;
+    T_.clear();
+    Y_.clear();
+    Integrator::clean();
+}

@@ -24,9 +24,12 @@ CELL_STATUS = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC",
 
 # Every symbol include/b200ode.h declares.
 EXPORTED = ["b200ode_default_options", "b200ode_create", "b200ode_destroy", "b200ode_num_species",
+            "b200ode_mechanism_species",
             "b200ode_integrate", "b200ode_integrate_device", "b200ode_integrate_device_noalloc",
             "b200ode_eval_rhs",
             "b200ode_eval_jacobian", "b200ode_fp64_peak",
+            "b200ode_default_server_options", "b200ode_server_create", "b200ode_server_destroy",
+            "b200ode_submit", "b200ode_poll", "b200ode_server_get_report",
             "b200ode_last_error", "b200ode_version"]
 
 
@@ -61,6 +64,25 @@ class Stats(C.Structure):
                 ("gpu_launches", C.c_int32), ("phase_cycles", C.c_int64 * 5)]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [("solver", Options), ("hbm_budget_bytes", C.c_int64), ("max_inflight", C.c_int32),
+                ("max_queued", C.c_int32)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("n_cells", C.c_int64), ("n_failed", C.c_int64), ("total_nst", C.c_int64),
+                ("total_nni", C.c_int64), ("footprint_bytes", C.c_int64), ("queue_ms", C.c_double),
+                ("device_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class ServerReport(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed_requests", C.c_int64),
+                ("cells_completed", C.c_int64), ("p50_latency_ms", C.c_double),
+                ("p99_latency_ms", C.c_double), ("max_latency_ms", C.c_double),
+                ("mean_queue_ms", C.c_double), ("cells_per_sec", C.c_double),
+                ("max_concurrent", C.c_int32), ("budget_bytes", C.c_int64), ("peak_bytes", C.c_int64)]
+
+
 COUNTERS = ["nst", "nfe", "nje", "nsetups", "nni", "ncfn", "netf"]
 _dp = C.POINTER(C.c_double)
 _lib: Optional[C.CDLL] = None
@@ -82,6 +104,8 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.b200ode_destroy.restype = None
     lib.b200ode_num_species.argtypes = [C.c_void_p]
     lib.b200ode_num_species.restype = C.c_int32
+    lib.b200ode_mechanism_species.argtypes = [C.c_char_p]
+    lib.b200ode_mechanism_species.restype = C.c_int32
     lib.b200ode_integrate.argtypes = [C.c_void_p, C.c_int64, _dp, C.c_double, _dp, _dp, C.c_double,
                                       C.c_double, _i32p, C.POINTER(Stats)]
     lib.b200ode_integrate.restype = C.c_int
@@ -97,6 +121,19 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.b200ode_eval_jacobian.restype = C.c_int
     lib.b200ode_fp64_peak.argtypes = [C.c_int32, C.POINTER(C.c_double)]
     lib.b200ode_fp64_peak.restype = C.c_int
+    lib.b200ode_default_server_options.argtypes = [C.POINTER(ServerOptions)]
+    lib.b200ode_default_server_options.restype = None
+    lib.b200ode_server_create.argtypes = [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]
+    lib.b200ode_server_create.restype = C.c_int
+    lib.b200ode_server_destroy.argtypes = [C.c_void_p]
+    lib.b200ode_server_destroy.restype = None
+    lib.b200ode_submit.argtypes = [C.c_void_p, C.c_char_p, C.c_int64, _dp, C.c_double, _dp, _dp,
+                                   C.c_double, C.c_double, _i32p, C.POINTER(C.c_uint64)]
+    lib.b200ode_submit.restype = C.c_int
+    lib.b200ode_poll.argtypes = [C.c_void_p, C.c_uint64, C.c_int32, C.POINTER(RequestInfo)]
+    lib.b200ode_poll.restype = C.c_int
+    lib.b200ode_server_get_report.argtypes = [C.c_void_p, C.POINTER(ServerReport)]
+    lib.b200ode_server_get_report.restype = C.c_int
     lib.b200ode_last_error.argtypes = []
     lib.b200ode_last_error.restype = C.c_char_p
     lib.b200ode_version.argtypes = []
@@ -218,6 +255,70 @@ class Solver:
             C.byref(st) if st is not None else None, C.c_void_p(stream or None)))
         self.last_stats = st
         return stats_dict(st) if st is not None else None
+
+
+B200ODE_ERR_NOT_READY = 7
+
+
+class Server:
+    """The request loop of the C ABI (b200ode_server_*): submit batches of cells,
+    poll for their results; continuous batching on one GPU."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 4, max_queued: int = 4096, **solver_kw):
+        self.lib = load()
+        o = ServerOptions()
+        self.lib.b200ode_default_server_options(C.byref(o))
+        for k, v in solver_kw.items():
+            if not hasattr(o.solver, k):
+                raise KeyError(k)
+            setattr(o.solver, k, v)
+        o.hbm_budget_bytes = int(hbm_budget_bytes)
+        o.max_inflight = int(max_inflight)
+        o.max_queued = int(max_queued)
+        h = C.c_void_p()
+        _check(self.lib.b200ode_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self._live = {}   # request id -> buffers the library writes into
+
+    def submit(self, mech: str, T: np.ndarray, Y: np.ndarray, P, t1: float, t0: float = 0.0) -> int:
+        """Queue cells (T[n], Y[nsp, n] SoA, updated in place when done)."""
+        n = T.size
+        assert T.dtype == np.float64 and T.flags.c_contiguous
+        assert Y.dtype == np.float64 and Y.flags.c_contiguous and Y.shape[1] == n
+        parr, ps = (None, float(P)) if np.ndim(P) == 0 else (np.ascontiguousarray(P, dtype=np.float64), 0.0)
+        status = np.full(n, 99, dtype=np.int32)
+        rid = C.c_uint64()
+        _check(self.lib.b200ode_submit(self.h, mech.encode(), n, _ptr(parr), ps, _ptr(T), _ptr(Y), float(t0),
+                                       float(t1), status.ctypes.data_as(_i32p), C.byref(rid)))
+        self._live[rid.value] = (T, Y, parr, status)
+        return rid.value
+
+    def poll(self, rid: int, wait_ms: int = -1):
+        """(status[n], info dict) when done, None if still in flight after wait_ms."""
+        info = RequestInfo()
+        rc = self.lib.b200ode_poll(self.h, rid, int(wait_ms), C.byref(info))
+        if rc == B200ODE_ERR_NOT_READY:
+            return None
+        bufs = self._live.pop(rid, None)
+        _check(rc)
+        return bufs[3], {f: getattr(info, f) for f, _ in RequestInfo._fields_}
+
+    def report(self) -> dict:
+        r = ServerReport()
+        _check(self.lib.b200ode_server_get_report(self.h, C.byref(r)))
+        return {f: getattr(r, f) for f, _ in ServerReport._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.b200ode_server_destroy(self.h)
+            self.h = None
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def fp64_peak_gflops(device: int = -1) -> float:

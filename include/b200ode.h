@@ -103,6 +103,11 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
                               b200ode_handle** out);
 void b200ode_destroy(b200ode_handle* h);
 
+/* Number of species of a mechanism by name, without a device (the reference's
+ * NSP, src/Mechanism/CPU/mechanism.h); -1 for an unknown name.  Lets a host
+ * check a mesh against the mechanism before any GPU work. */
+int32_t b200ode_mechanism_species(const char* mech_name);
+
 /* Number of species of the handle's mechanism (the reference's NSP). */
 int32_t b200ode_num_species(const b200ode_handle* h);
 
@@ -185,6 +190,72 @@ b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n_cells, const d
  * denominator of the FP64-pipe roofline this library reports.  No reference
  * counterpart (a measurement helper). */
 b200ode_status b200ode_fp64_peak(int32_t device, double* gflops);
+
+/* ------------------------------------------------------------------ serving
+ * A request loop for an operator-split flow solver that sends chemistry batches
+ * (different sizes, different mechanisms) every flow step.  No counterpart in the
+ * reference, whose integrators are synchronous (Integrator::integrate,
+ * Integrator.hpp:22-40); the per-request work is exactly b200ode_integrate's.
+ *
+ * Continuous batching: a host thread admits queued requests as soon as a
+ * stream slot is free and the request's device footprint fits in what is free
+ * of the server's device budget (reserved once at creation; admission is
+ * bookkeeping, no cudaMalloc while kernels run).  Admitted requests run on
+ * their own streams, so their kernels overlap on the GPU: thread blocks of a
+ * later request take SMs as those of earlier requests finish.  Admission is
+ * first-in first-out; a request that does not fit lets smaller later ones pass
+ * at most 8 times before the queue waits for it.  Each cell's result does not
+ * depend on what else is in flight. */
+typedef struct b200ode_server b200ode_server;
+
+typedef struct {
+    b200ode_options solver;     /* tolerances, precision, launch shape of every request */
+    int64_t hbm_budget_bytes;   /* device bytes requests in flight may hold (0 = 25 % of free memory) */
+    int32_t max_inflight;       /* requests on the GPU at once = streams (0 = 4) */
+    int32_t max_queued;         /* requests waiting for admission before submit returns BUSY (0 = 4096) */
+} b200ode_server_options;
+
+typedef struct {
+    int64_t n_cells;
+    int64_t n_failed;          /* cells whose status != B200ODE_CELL_SUCCESS */
+    int64_t total_nst, total_nni;
+    int64_t footprint_bytes;   /* device bytes the request held while in flight */
+    double queue_ms;           /* submit -> admitted */
+    double device_ms;          /* H2D + kernel + D2H on its stream (CUDA events) */
+    double latency_ms;         /* submit -> results in the caller's buffers */
+} b200ode_request_info;
+
+typedef struct {
+    int64_t submitted, completed, failed_requests, cells_completed;
+    double p50_latency_ms, p99_latency_ms, max_latency_ms, mean_queue_ms;
+    double cells_per_sec;          /* completed cells / (last completion - first submit) */
+    int32_t max_concurrent;        /* most requests in flight at once */
+    int64_t budget_bytes, peak_bytes;
+} b200ode_server_report;
+
+void b200ode_default_server_options(b200ode_server_options* opts);
+b200ode_status b200ode_server_create(const b200ode_server_options* opts, b200ode_server** out);
+/* Waits for requests in flight; requests still queued are dropped. */
+void b200ode_server_destroy(b200ode_server* s);
+
+/* Queue one batch: arguments as b200ode_integrate (host buffers).  T, Y and
+ * cell_status (may be NULL) receive the results; P, T, Y and cell_status must
+ * stay valid and untouched until b200ode_poll reports the request done.
+ * Returns B200ODE_ERR_BUSY when max_queued requests wait, B200ODE_ERR_INVALID
+ * when the request alone exceeds the server's device budget. */
+b200ode_status b200ode_submit(b200ode_server* s, const char* mech_name, int64_t n_cells, const double* P,
+                              double P_scalar, double* T, double* Y, double t0, double t1,
+                              int32_t* cell_status, uint64_t* request_id);
+
+/* B200ODE_OK when the request is done (results in the caller's buffers, info
+ * filled if non-NULL, the id retired); B200ODE_ERR_NOT_READY if it is still
+ * queued or running after waiting up to wait_ms (0 = do not wait, -1 = until
+ * done); another status if the request failed (message in b200ode_last_error). */
+b200ode_status b200ode_poll(b200ode_server* s, uint64_t request_id, int32_t wait_ms,
+                            b200ode_request_info* info);
+
+/* Latency percentiles and throughput over the requests completed so far. */
+b200ode_status b200ode_server_get_report(b200ode_server* s, b200ode_server_report* report);
 
 /* Message of the last error on this thread ("" if none). */
 const char* b200ode_last_error(void);

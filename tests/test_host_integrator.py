@@ -1,0 +1,77 @@
+"""The C++ host integrator (B200BDFIntegrator behind the restated reference
+Integrator interface, include/b200ode_integrator.hpp): factory selection, the
+reference's mechanism-size check, error behaviour -- on the CPU; results on the
+GPU (marked gpu) against the reference's quiescent case and the C ABI."""
+import numpy as np
+import pytest
+
+import host_driver
+from hpc_ode_b200 import native, workloads as W
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    d = tmp_path_factory.mktemp("hostdrv")
+    return host_driver.build(d), d
+
+
+def _cells(n=4, nsp=53):
+    T = np.full(n, 1200.0)
+    Y = np.full((n, nsp), 1.0 / nsp)
+    return T, Y
+
+
+def test_unknown_integrator_type(driver):
+    exe, d = driver
+    T, Y = _cells()
+    rc, out, *_ = host_driver.run(exe, d, "CVodeIntegratorGPU", "gri30.yaml", T, Y, 1e-6, 101325.0)
+    assert rc == 3 and "Integrator type is not valid" in out
+
+
+def test_mechanism_size_mismatch_throws_before_device_work(driver):
+    exe, d = driver
+    T, Y = _cells(nsp=10)
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0)
+    assert rc == 3 and "mechanism size of: gri30.yaml (53) differs from the mesh size: 10" in out
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "nDodecane_Reitz.yaml", T, Y, 1e-6, 101325.0)
+    assert rc == 3 and "(-1) differs" in out
+
+
+def test_no_device_is_a_runtime_error(driver):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    exe, d = driver
+    T, Y = _cells()
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0)
+    assert rc == 3 and "no CUDA device" in out
+
+
+@pytest.mark.gpu
+def test_quiescent_reference_case_through_cpp(driver, golden_e2e):
+    exe, d = driver
+    g = golden_e2e
+    rc, out, To, Yo, st = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", g["T_in"], g["Y_in"],
+                                          float(g["dt"]), float(g["P"]))
+    assert rc == 0, out
+    assert "B200BDFIntegrator initialized" in out and "Integrator clean completed" in out
+    assert (st == 0).all()
+    assert np.abs(To - g["T_out"]).max() <= 1e-9 * 300
+    assert np.abs(Yo[:, :-1] - g["Y_out"][:, :-1]).max() <= 1e-20
+    assert np.abs(Yo[:, -1] - g["Y_out"][:, -1]).max() <= 1e-15
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wl,mech", [("gri_32k", "gri30.yaml"), ("h2_1024", "h2o2.yaml")])
+def test_reacting_cells_match_c_abi(driver, wl, mech):
+    exe, d = driver
+    b = W.make(wl, 48, seed=77)
+    P = float(b.P[0])
+    rc, out, To, Yo, st = host_driver.run(exe, d, "BDFIntegratorB200", mech, b.T, b.Y.T, b.dt, P)
+    assert rc == 0, out
+    s = native.Solver(b.mech)
+    T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+    st2, _, _ = s.integrate(T, Y, P, b.dt)
+    s.close()
+    assert np.array_equal(st, st2)
+    assert np.array_equal(To, T) and np.array_equal(Yo, Y.T)
