@@ -155,6 +155,31 @@ def run_reference_arm(args):
     return 0
 
 
+def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample: int = 256) -> dict:
+    """Error of the GPU result against the FP64 oracle (the CVODE-semantics BDF
+    at rtol 1e-10 / atol 1e-14) on a stratified sample of cells, beside the
+    error of the CPU integrator at the same rtol/atol as the GPU."""
+    from oracle import pyoracle
+    o = pyoracle.get()
+    n = batch.ncells
+    idx = np.arange(0, n, max(1, n // nsample))[:nsample]
+    sub = batch.subset(idx)
+    threads = os.cpu_count() or 1
+    ytrue, st_true = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=1e-10, atol=1e-14, threads=threads)
+    ycpu, _ = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=W.RTOL, atol=W.ATOL, threads=threads)
+    Tg, Yg = T_gpu[idx], Y_gpu[:-1, idx].T
+    eT = np.abs(Tg - ytrue[:, 0]) / ytrue[:, 0]
+    eTc = np.abs(ycpu[:, 0] - ytrue[:, 0]) / ytrue[:, 0]
+    okY = np.abs(Yg - ytrue[:, 1:]) <= np.maximum(1e-4 * np.abs(ytrue[:, 1:]), 1e-10)
+    okYc = np.abs(ycpu[:, 1:] - ytrue[:, 1:]) <= np.maximum(1e-4 * np.abs(ytrue[:, 1:]), 1e-10)
+    return {"oracle": "CVODE-semantics BDF, FP64, rtol 1e-10 atol 1e-14", "cells": int(idx.size),
+            "gpu_T_rel_max": float(eT.max()), "gpu_T_rel_p99": float(np.quantile(eT, 0.99)),
+            "gpu_Y_within_gate": float(okY.mean()),
+            "cpu_T_rel_max": float(eTc.max()), "cpu_Y_within_gate": float(okYc.mean()),
+            "gate": "|dT|/T <= 1e-5; |dY| <= max(1e-4 |Y|, 1e-10)",
+            "oracle_failed": int((st_true["status"] != 0).sum())}
+
+
 def fp64_peak_gflops(torch, native_mod) -> float:
     """Measured FP64 FMA throughput of this GPU (library microkernel), GFLOP/s."""
     try:
@@ -177,6 +202,7 @@ def main():
                     help="cells of the workload the CPU baseline integrates per step (stratified)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -315,6 +341,13 @@ def main():
     except Exception as e:  # noqa: BLE001
         fp64 = {"error": str(e)}
 
+    acc = None
+    if rank == 0 and not args.no_accuracy:
+        try:
+            acc = accuracy_block(batch, T.cpu().numpy(), Y.cpu().numpy())
+        except Exception as e:  # noqa: BLE001
+            acc = {"error": str(e)}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         ncpu, el, kind, what, _ = cpu_reference(batch, args.cpu_sample, os.cpu_count() or 1)
@@ -341,6 +374,7 @@ def main():
         "roofline": roofline,
         "fp64": fp64,
         "cpu_baseline": cpu,
+        "accuracy": acc,
         "clocks": clk,
     }
     if rank == 0:
