@@ -175,39 +175,46 @@ __device__ __noinline__ void bdf_adjust_order(unsigned off, int dq, int lane) {
     const int q = S.q;
     if (q == 2 && dq != 1) return;
     double* l = S.l;
+    #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j) l[j] = 0.0;
     l[2] = 1.0;
     if (dq == 1) {
         double alpha1 = 1.0, prod = 1.0, xiold = 1.0, alpha0 = -1.0, hsum = S.hscale;
+        #pragma unroll 1
         for (int j = 1; j < q; ++j) {
             hsum += S.tau[j + 1];
-            const double xi = hsum / S.hscale;
+            const double xi = ode_div(hsum, S.hscale);
             prod *= xi;
-            alpha0 -= 1.0 / (j + 1);
-            alpha1 += 1.0 / xi;
+            alpha0 -= ode_div(1.0, (double)(j + 1));
+            alpha1 += ode_div(1.0, xi);
+            #pragma unroll 1
             for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xiold + l[i - 1];
             xiold = xi;
         }
-        const double A1 = (-alpha0 - alpha1) / prod;
+        const double A1 = ode_div(-alpha0 - alpha1, prod);
         const int L = S.L, ia = S.indx_acor;
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) {
             const int i = lane + 32 * s;
             const double col = A1 * w->zn[ia][i];
             w->zn[L][i] = col;
+            #pragma unroll 1
             for (int j = 2; j <= q; ++j) w->zn[j][i] += l[j] * col;
         }
     } else if (dq == -1) {
         double hsum = 0.0;
+        #pragma unroll 1
         for (int j = 1; j <= q - 2; ++j) {
             hsum += S.tau[j];
-            const double xi = hsum / S.hscale;
+            const double xi = ode_div(hsum, S.hscale);
+            #pragma unroll 1
             for (int i = j + 2; i >= 2; --i) l[i] = l[i] * xi + l[i - 1];
         }
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) {
             const int i = lane + 32 * s;
             const double zq = w->zn[q][i];
+            #pragma unroll 1
             for (int j = 2; j < q; ++j) w->zn[j][i] += -l[j] * zq;
         }
     }
@@ -225,48 +232,52 @@ __device__ __noinline__ void bdf_set_coeffs(unsigned off) {
     const double h = S.h;
     l[0] = l[1] = 1.0;
     double xi_inv = 1.0, xistar_inv = 1.0;
+    #pragma unroll 1
     for (int j = 2; j <= cv::QMAX; ++j) l[j] = 0.0;
     double alpha0 = -1.0, alpha0_hat = -1.0, hsum = h;
     if (q > 1) {
+        #pragma unroll 1
         for (int j = 2; j < q; ++j) {
             hsum += tau[j - 1];
-            xi_inv = h / hsum;
-            alpha0 -= 1.0 / j;
+            xi_inv = ode_div(h, hsum);
+            alpha0 -= ode_div(1.0, (double)j);
+            #pragma unroll 1
             for (int i = j; i >= 1; --i) l[i] += l[i - 1] * xi_inv;
         }
-        alpha0 -= 1.0 / q;
+        alpha0 -= ode_div(1.0, (double)q);
         xistar_inv = -l[1] - alpha0;
         hsum += tau[q - 1];
-        xi_inv = h / hsum;
+        xi_inv = ode_div(h, hsum);
         alpha0_hat = -l[1] - xi_inv;
+        #pragma unroll 1
         for (int i = q; i >= 1; --i) l[i] += l[i - 1] * xistar_inv;
     }
     const double A1 = 1.0 - alpha0_hat + alpha0;
     const double A2 = 1.0 + q * A1;
-    tq[2] = fabs(A1 / (alpha0 * A2));
-    tq[5] = fabs(A2 * xistar_inv / (l[q] * xi_inv));
+    tq[2] = fabs(ode_div(A1, alpha0 * A2));
+    tq[5] = fabs(ode_div(A2 * xistar_inv, l[q] * xi_inv));
     if (S.qwait == 1) {
         if (q > 1) {
-            const double C = xistar_inv / l[q];
-            const double A3 = alpha0 + 1.0 / q;
+            const double C = ode_div(xistar_inv, l[q]);
+            const double A3 = alpha0 + ode_div(1.0, (double)q);
             const double A4 = alpha0_hat + xi_inv;
-            const double Cpinv = (1.0 - A4 + A3) / A3;
+            const double Cpinv = ode_div(1.0 - A4 + A3, A3);
             tq[1] = fabs(C * Cpinv);
         } else {
             tq[1] = 1.0;
         }
         hsum += tau[q];
-        xi_inv = h / hsum;
-        const double A5 = alpha0 - 1.0 / (q + 1);
+        xi_inv = ode_div(h, hsum);
+        const double A5 = alpha0 - ode_div(1.0, (double)(q + 1));
         const double A6 = alpha0_hat - xi_inv;
-        const double Cppinv = (1.0 - A6 + A5) / A2;
-        tq[3] = fabs(Cppinv / (xi_inv * (q + 2) * A5));
+        const double Cppinv = ode_div(1.0 - A6 + A5, A2);
+        tq[3] = fabs(ode_div(Cppinv, xi_inv * (q + 2) * A5));
     }
-    tq[4] = cv::NLSCOEF / tq[2];
-    S.rl1 = 1.0 / l[1];
+    tq[4] = ode_div(cv::NLSCOEF, tq[2]);
+    S.rl1 = ode_div(1.0, l[1]);
     S.gamma = h * S.rl1;
     if (S.nst == 0) S.gammap = S.gamma;
-    S.gamrat = (S.nst > 0) ? S.gamma / S.gammap : 1.0;
+    S.gamrat = (S.nst > 0) ? ode_div(S.gamma, S.gammap) : 1.0;
 }
 
 // Linear-solver setup (CVODE's cvNlsLSetup + cvLsSetup): Jacobian reuse
@@ -279,7 +290,7 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
     BdfState& S = w->st;
     if (jbad_in) S.convfail = cv::FAIL_BAD_J;
     const int cf = S.convfail;
-    const double dgamma = fabs(S.gamma / S.gammap - 1.0);
+    const double dgamma = fabs(ode_div(S.gamma, S.gammap) - 1.0);
     const bool jbad = (S.nst == 0) || (S.nst >= S.nstlj + cv::MSBJ) ||
                       ((cf == cv::FAIL_BAD_J) && (dgamma < cv::DGMAX_JBAD)) || (cf == cv::FAIL_OTHER);
     LinT* A = w->A;
@@ -288,6 +299,7 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
         S.jcur = 0;
 #pragma unroll 1
         for (int i = 0; i < N; ++i)
+            #pragma unroll 1
             for (int j = lane; j < N; j += 32) A[i * LDA + j] = J[i * N + j];
     } else {
         S.cnt[C_NJE]++;
@@ -298,12 +310,14 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
         ph_tock(S, PH_JAC, tj, lane);
 #pragma unroll 1
         for (int i = 0; i < N; ++i)
+            #pragma unroll 1
             for (int j = lane; j < N; j += 32) J[i * N + j] = A[i * LDA + j];
     }
     __syncwarp();
     const LinT mg = (LinT)(-S.gamma);
 #pragma unroll 1
     for (int i = 0; i < N; ++i)
+        #pragma unroll 1
         for (int j = lane; j < N; j += 32) {
             LinT v = mg * A[i * LDA + j];
             if (i == j) v += LinT(1);
@@ -356,7 +370,7 @@ __device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], con
         for (int s = 0; s < NS; ++s) x.v[s] += d.v[s];
     }
     const double gamrat = S.gamrat;
-    const double sc = (gamrat != 1.0) ? 2.0 / (1.0 + gamrat) : 1.0;
+    const double sc = (gamrat != 1.0) ? ode_div(2.0, 1.0 + gamrat) : 1.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) b[s] = (gamrat != 1.0) ? x.v[s] * sc : x.v[s];
     ph_tock(S, PH_SOLVE, t0, lane);
@@ -378,7 +392,7 @@ __device__ __noinline__ void bdf_prepare_next_step(unsigned off, double dsm, con
         S.eta = 1.0;
         return;
     }
-    S.etaq = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / L) + cv::ADDON);
+    S.etaq = ode_div(1.0, ode_pow(cv::BIAS2 * dsm, ode_div(1.0, (double)L)) + cv::ADDON);
     double eta;
     int qprime = q;
     if (S.qwait != 0) {
@@ -388,15 +402,15 @@ __device__ __noinline__ void bdf_prepare_next_step(unsigned off, double dsm, con
         double etaqm1 = 0.0, etaqp1 = 0.0;
         if (q > 1) {
             const double ddn = wrms_zn<MT, LinT>(w, q, ewv.v, lane) * S.tq[1];
-            etaqm1 = 1.0 / (pow(cv::BIAS1 * ddn, 1.0 / q) + cv::ADDON);
+            etaqm1 = ode_div(1.0, ode_pow(cv::BIAS1 * ddn, ode_div(1.0, (double)q)) + cv::ADDON);
         }
         if (q != S.qmax && S.saved_tq5 != 0.0) {
-            const double cquot = (S.tq[5] / S.saved_tq5) * pow(S.h / S.tau[2], (double)L);
+            const double cquot = ode_div(S.tq[5], S.saved_tq5) * ode_pow(ode_div(S.h, S.tau[2]), (double)L);
             double tmp[NS];
 #pragma unroll
             for (int s = 0; s < NS; ++s) tmp[s] = acv.v[s] - cquot * w->zn[S.qmax][lane + 32 * s];
             const double dup = wrms_v<NS>(tmp, ewv.v, MT::N) * S.tq[3];
-            etaqp1 = 1.0 / (pow(cv::BIAS3 * dup, 1.0 / (L + 1)) + cv::ADDON);
+            etaqp1 = ode_div(1.0, ode_pow(cv::BIAS3 * dup, ode_div(1.0, (double)(L + 1))) + cv::ADDON);
         }
         S.etaqm1 = etaqm1;
         S.etaqp1 = etaqp1;
@@ -440,7 +454,7 @@ __device__ __noinline__ int bdf_error_fail(unsigned off, double dsm, double save
     if (nef == cv::MXNEF) return cv::CV_ERR_FAILURE;
     S.etamax = 1.0;
     if (nef <= cv::MXNEF1) {
-        double eta = 1.0 / (pow(cv::BIAS2 * dsm, 1.0 / S.L) + cv::ADDON);
+        double eta = ode_div(1.0, ode_pow(cv::BIAS2 * dsm, ode_div(1.0, (double)S.L)) + cv::ADDON);
         eta = fmax(cv::ETAMIN, eta);
         if (nef >= cv::SMALL_NEF) eta = fmin(eta, cv::ETAMXF);
         S.eta = eta;
@@ -480,7 +494,9 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
         for (int s = 0; s < NS; ++s) w->zn[j][lane + 32 * s] = (j == 0 && valid_el<NS>(lane, s, N)) ? y0.v[s] : 0.0;
+    #pragma unroll 1
     for (int j = 0; j < 8; ++j) S.l[j] = S.tq[j] = S.tau[j] = 0.0;
+    #pragma unroll 1
     for (int j = 0; j < 7; ++j) S.cnt[j] = 0;
     S.tn = t0;
     S.q = 1; S.L = 2; S.qwait = 2; S.qprime = 1;
@@ -511,30 +527,31 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
 #pragma unroll
     for (int s = 0; s < NS; ++s)
         if (valid_el<NS>(lane, s, N)) {
-            const double den = cv::HUB_FACTOR * fabs(z0[s]) + 1.0 / ewt[s];
-            r = fmax(r, fabs(z1[s]) / den);
+            const double den = cv::HUB_FACTOR * fabs(z0[s]) + ode_div(1.0, ewt[s]);
+            r = fmax(r, ode_div(fabs(z1[s]), den));
         }
     const double hub_inv = warp_max(r);
     double hub = cv::HUB_FACTOR * tdist;
-    if (hub * hub_inv > 1.0) hub = 1.0 / hub_inv;
+    if (hub * hub_inv > 1.0) hub = ode_div(1.0, hub_inv);
     double hg = sqrt(hlb * hub);
     double h0;
     if (hub < hlb) {
         h0 = sign * hg;
     } else {
         double hnew = hg;
+        #pragma unroll 1
         for (int count1 = 1; count1 <= cv::MAX_HIN_ITERS; ++count1) {
             const double hgs = hg * sign;
 #pragma unroll
             for (int s = 0; s < NS; ++s) y[s] = hgs * z1[s] + z0[s];
             bdf_rhs<MT, LinT>(off, y, tmp, lane);
-            const double ih = 1.0 / hgs;
+            const double ih = ode_div(1.0, hgs);
 #pragma unroll
             for (int s = 0; s < NS; ++s) tmp[s] = (tmp[s] - z1[s]) * ih;
             const double yddnrm = wrms_v<NS>(tmp, ewt, N);
-            hnew = (yddnrm * hub * hub > 2.0) ? sqrt(2.0 / yddnrm) : sqrt(hg * hub);
+            hnew = (yddnrm * hub * hub > 2.0) ? sqrt(ode_div(2.0, yddnrm)) : sqrt(hg * hub);
             if (count1 == cv::MAX_HIN_ITERS) break;
-            const double hrat = hnew / hg;
+            const double hrat = ode_div(hnew, hg);
             if (hrat > 0.5 && hrat < 2.0) break;
             if (count1 > 1 && hrat > 2.0) { hnew = hg; break; }
             hg = hnew;
@@ -560,9 +577,10 @@ __device__ __noinline__ Vec<MT::NS> bdf_finish(unsigned off, int status, double 
     BdfState& S = w->st;
     Vec<MT::NS> out;
     if (status == 0) {
-        const double s_ = (tout - S.tn) / S.h;
+        const double s_ = ode_div(tout - S.tn, S.h);
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[S.q][lane + 32 * s];
+        #pragma unroll 1
         for (int j = S.q - 1; j >= 0; --j)
 #pragma unroll
             for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[j][lane + 32 * s] + s_ * out.v[s];
@@ -646,8 +664,8 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
 #pragma unroll
                     for (int s = 0; s < NS; ++s) acor[s] += delta[s];
                     const double del = wrms_v<NS>(delta, ewt, N);
-                    if (m > 0) S.crate = fmax(cv::CRDOWN * S.crate, del / delp);
-                    const double dcon = del * fmin(1.0, S.crate) / S.tq[4];
+                    if (m > 0) S.crate = fmax(cv::CRDOWN * S.crate, ode_div(del, delp));
+                    const double dcon = ode_div(del * fmin(1.0, S.crate), S.tq[4]);
                     if (dcon <= 1.0) {
                         S.acnrm = (m == 0) ? del : wrms_v<NS>(acor, ewt, N);
                         S.jcur = 0;
@@ -702,6 +720,7 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
             S.hu = S.h;
             {
                 const int q = S.q;
+                #pragma unroll 1
                 for (int i = q; i >= 2; --i) S.tau[i] = S.tau[i - 1];
                 if (q == 1 && S.nst > 1) S.tau[2] = S.tau[1];
                 S.tau[1] = S.h;
@@ -761,6 +780,7 @@ __device__ __noinline__ void bdf_save(unsigned off, unsigned char* rec, int phas
     for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
     if (lane == 0) *reinterpret_cast<int*>(rec + R::kPhaseOff) = phase;
     double* Z = reinterpret_cast<double*>(rec + R::kStateBytes + 8);
+    #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s)
@@ -769,8 +789,10 @@ __device__ __noinline__ void bdf_save(unsigned off, unsigned char* rec, int phas
         LinT* Ag = reinterpret_cast<LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
         for (int e = lane; e < N * MT::LDA; e += 32) Ag[e] = w->A[e];
+        #pragma unroll 1
         for (int e = lane; e < N; e += 32) Ag[N * MT::LDA + e] = w->dinv[e];
         int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA + N);
+        #pragma unroll 1
         for (int e = lane; e < N; e += 32) pg[e] = w->perm[e];
     }
     __syncwarp();
@@ -786,6 +808,7 @@ __device__ __noinline__ void bdf_load(unsigned off, const unsigned char* rec, in
 #pragma unroll 1
     for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
     const double* Z = reinterpret_cast<const double*>(rec + R::kStateBytes + 8);
+    #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s)
@@ -793,8 +816,10 @@ __device__ __noinline__ void bdf_load(unsigned off, const unsigned char* rec, in
     const LinT* Ag = reinterpret_cast<const LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
     for (int e = lane; e < N * MT::LDA; e += 32) w->A[e] = Ag[e];
+    #pragma unroll 1
     for (int e = lane; e < N; e += 32) w->dinv[e] = Ag[N * MT::LDA + e];
     const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA + N);
+    #pragma unroll 1
     for (int e = lane; e < N; e += 32) w->perm[e] = pg[e];
     __syncwarp();
 }

@@ -172,6 +172,18 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     return c;
 }
 
+// Out-of-line FP64 transcendentals: one copy of each library routine in the
+// kernel image instead of one per call site.  The integration kernel is bound
+// by instruction fetch (its hot code is larger than the SM's instruction
+// cache), so every call site that is not a full inline expansion helps.
+__device__ __noinline__ double ode_exp(double x) { return exp(x); }
+__device__ __noinline__ double ode_log10(double x) { return log10(x); }
+__device__ __noinline__ double ode_exp10(double x) { return exp10(x); }
+__device__ __noinline__ double ode_pow(double x, double y) { return pow(x, y); }
+// IEEE division out of line: an inline FP64 division is ~40 instructions, so
+// the scalar step-control code calls this single copy instead.
+__device__ __noinline__ double ode_div(double a, double b) { return a / b; }
+
 // Rates of one reaction slot.  With Deriv, also the pieces of its derivative.
 struct RxnOut {
     double q;            // (Rf - Rr) * phi
@@ -187,9 +199,8 @@ struct FallOut {
     double phi, dphi_dthd, dphi_dT;
 };
 
-template <bool Deriv>
 __device__ __noinline__ FallOut falloff(int mech_id, int s, int fl, double T, double logT, double invT,
-                                        double kf, double thd) {
+                                        double kf, double thd, int Deriv) {
     const DevMech& M = c_mech[mech_id];
     const int type = fl & kFlagTypeMask;
     struct { double T, logT, invT; } c = {T, logT, invT};
@@ -199,51 +210,63 @@ __device__ __noinline__ FallOut falloff(int mech_id, int s, int fl, double T, do
     const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
     const double b0 = __ldg(M.b0 + s), EaR0 = __ldg(M.EaR0 + s);
     const double k0 = (fl & kFlagConstK0) ? __ldg(M.A0const + s)
-                                          : exp(__ldg(M.logA0 + s) + b0 * c.logT - EaR0 * c.invT);
-    const double Pr = k0 * thd / kf;
+                                          : ode_exp(__ldg(M.logA0 + s) + b0 * c.logT - EaR0 * c.invT);
+    const double Pr = ode_div(k0 * thd, kf);
     double F = 1.0, dl_dx = 0.0, dl_dT = 0.0;
     if (type == 3) {
         const double a = __ldg(M.troe_a + s), iT3 = __ldg(M.troe_iT3 + s), iT1 = __ldg(M.troe_iT1 + s);
-        const double e3 = exp(-c.T * iT3), e1 = exp(-c.T * iT1);
+        const double e3 = ode_exp(-c.T * iT3), e1 = ode_exp(-c.T * iT1);
         double Fcent = (1.0 - a) * e3 + a * e1;
         double dFcent = 0.0;
         if (Deriv) dFcent = -(1.0 - a) * iT3 * e3 - a * iT1 * e1;
         if (fl & kFlagT2) {
             const double T2 = __ldg(M.troe_T2 + s);
-            const double e2 = exp(-T2 * c.invT);
+            const double e2 = ode_exp(-T2 * c.invT);
             Fcent += e2;
             if (Deriv) dFcent += T2 * c.invT * c.invT * e2;
         }
-        const double Fc = log10(fmax(Fcent, 1.0e-300));
-        const double x = log10(fmax(Pr, 1.0e-300));
+        const double Fc = ode_log10(fmax(Fcent, 1.0e-300));
+        const double x = ode_log10(fmax(Pr, 1.0e-300));
         const double A = x - 0.67 * Fc - 0.4;
         const double B = 0.806 - 1.1762 * Fc - 0.14 * x;
-        const double u = A / B;
+        const double u = ode_div(A, B);
         const double den = 1.0 + u * u;
-        F = exp10(Fc / den);
+        F = ode_exp10(ode_div(Fc, den));
         if (Deriv) {
-            const double du_dx = (B + 0.14 * A) / (B * B);
-            const double du_dFc = (-0.67 * B + 1.1762 * A) / (B * B);
-            dl_dx = (Pr > 1.0e-300) ? -Fc * 2.0 * u * du_dx / (den * den) : 0.0;
-            const double dl_dFc = 1.0 / den - Fc * 2.0 * u * du_dFc / (den * den);
-            const double dFc_dT = (Fcent > 1.0e-300) ? dFcent / (Fcent * 2.302585092994046) : 0.0;
+            const double du_dx = ode_div(B + 0.14 * A, B * B);
+            const double du_dFc = ode_div(-0.67 * B + 1.1762 * A, B * B);
+            dl_dx = (Pr > 1.0e-300) ? ode_div(-Fc * 2.0 * u * du_dx, den * den) : 0.0;
+            const double dl_dFc = ode_div(1.0, den) - ode_div(Fc * 2.0 * u * du_dFc, den * den);
+            const double dFc_dT = (Fcent > 1.0e-300) ? ode_div(dFcent, Fcent * 2.302585092994046) : 0.0;
             dl_dT = dl_dFc * dFc_dT;
         }
     }
-    const double blend = Pr / (1.0 + Pr);
+    const double blend = ode_div(Pr, 1.0 + Pr);
     o.phi = F * blend;
     if (Deriv) {
-        const double dphi_dPr = F / ((1.0 + Pr) * (1.0 + Pr)) + F / (1.0 + Pr) * dl_dx;
-        o.dphi_dthd = dphi_dPr * (k0 / kf);
+        const double dphi_dPr = ode_div(F, (1.0 + Pr) * (1.0 + Pr)) + ode_div(F, 1.0 + Pr) * dl_dx;
+        o.dphi_dthd = dphi_dPr * ode_div(k0, kf);
         const double dlnPr_dT = (b0 + EaR0 * c.invT) * c.invT - (b + EaR * c.invT) * c.invT;
         o.dphi_dT = dphi_dPr * Pr * dlnPr_dT + blend * F * 2.302585092994046 * dl_dT;
     }
     return o;
 }
 
-template <bool Deriv>
-__device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int mech_id, int s, const CellThermo& c,
-                                           const double* C, const double* G) {
+// Cell quantities the reaction phase needs (passed by value to the
+// out-of-line slot evaluation).
+struct RxnCtx {
+    double T, logT, invT, m, mC;
+};
+
+// Rates of reaction slot s; with deriv, also the pieces of its derivative.
+// Out of line and shared by the RHS and the Jacobian: one copy of the reaction
+// code in the instruction cache.  C_off / G_off: shared-memory byte offsets of
+// the concentrations and -g/RT (index N holds the padding entries).
+__device__ __noinline__ RxnOut rxn_slot(int mech_id, int s, const RxnCtx c, unsigned C_off, unsigned G_off,
+                                        int deriv) {
+    const DevMech& M = c_mech[mech_id];
+    const double* C = smem_at<double>(C_off);
+    const double* G = smem_at<double>(G_off);
     RxnOut o;
     o.q = 0.0; o.kf = 0.0; o.kr = 0.0; o.Rf = 0.0; o.Rr = 0.0; o.phi = 1.0; o.thd = 0.0;
     o.dphi_dthd = 0.0; o.dphi_dT = 0.0; o.dlnkf_dT = 0.0;
@@ -253,16 +276,16 @@ __device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int mech_id, int s,
     const int r0 = __ldg(M.rf + s), r1 = __ldg(M.rf + ns + s), r2 = __ldg(M.rf + 2 * ns + s);
     const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
     const double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
-    const double kf = (fl & kFlagConstK) ? __ldg(M.Aconst + s) : exp(lkf);
+    const double kf = (fl & kFlagConstK) ? __ldg(M.Aconst + s) : ode_exp(lkf);
     o.kf = kf;
     o.Rf = kf * ((C[r0] * C[r1]) * C[r2]);
-    if (Deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
+    if (deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
     if (fl & kFlagRev) {
         const int p0 = __ldg(M.pf + s), p1 = __ldg(M.pf + ns + s), p2 = __ldg(M.pf + 2 * ns + s);
         const int dnu = __ldg(M.dnu + s);
         const double sg = (G[p0] + G[p1] + G[p2]) - (G[r0] + G[r1] + G[r2]);
         const double lnKc = sg - dnu * c.logT + __ldg(M.lnPfac + s);
-        const double kr = (fl & kFlagConstK) ? __ldg(M.Aconst + s) * exp(-lnKc) : exp(lkf - lnKc);
+        const double kr = (fl & kFlagConstK) ? __ldg(M.Aconst + s) * ode_exp(-lnKc) : ode_exp(lkf - lnKc);
         o.kr = kr;
         o.Rr = kr * ((C[p0] * C[p1]) * C[p2]);
     }
@@ -282,7 +305,7 @@ __device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int mech_id, int s,
             o.phi = thd;
             o.dphi_dthd = 1.0;
         } else {
-            const FallOut f = falloff<Deriv>(mech_id, s, fl, c.T, c.logT, c.invT, kf, thd);
+            const FallOut f = falloff(mech_id, s, fl, c.T, c.logT, c.invT, kf, thd, deriv);
             o.phi = f.phi;
             o.dphi_dthd = f.dphi_dthd;
             o.dphi_dT = f.dphi_dT;
@@ -292,15 +315,21 @@ __device__ __forceinline__ RxnOut rxn_eval(const DevMech& M, int mech_id, int s,
     return o;
 }
 
+__device__ __forceinline__ RxnCtx rxn_ctx(const CellThermo& c) { return RxnCtx{c.T, c.logT, c.invT, c.m, c.mC}; }
+
 // Balanced gather: out[s] = sum over species (lane + 32 s)'s (slot, nu) pairs of
-// nu * src[slot].  Unit partial sums go through sm->part.
-template <class MT>
-__device__ __forceinline__ void gather(const DevMech& M, const double* src, ChemSmem<MT>* sm, int lane,
-                                       double (&out)[MT::NS]) {
+// nu * src[slot]; src is the shared-memory array at byte offset src_off, or,
+// with kGlobal, the global array gsrc.  Unit partial sums go through the
+// chemistry scratch's part[].  Out of line: the RHS and the Jacobian share it.
+template <class MT, bool kGlobal>
+__device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off, unsigned chem_off, int lane) {
+    const DevMech& M = mech<MT>();
+    const double* src = kGlobal ? gsrc : smem_at<double>(src_off);
+    ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
     double acc = 0.0;
     const int gmax = M.gmax;
     const int* gw = M.gword + lane;
-#pragma unroll 4
+#pragma unroll 2
     for (int e = 0; e < gmax; ++e) {
         const int w = __ldg(gw + 32 * e);
         acc += (double)(((w >> 11) & 31) - 16) * src[w & 2047];
@@ -309,6 +338,7 @@ __device__ __forceinline__ void gather(const DevMech& M, const double* src, Chem
         acc = last ? 0.0 : acc;
     }
     __syncwarp();
+    Vec<MT::NS> out;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
         const int i = lane + 32 * s;
@@ -317,9 +347,10 @@ __device__ __forceinline__ void gather(const DevMech& M, const double* src, Chem
             const int u0 = __ldg(M.unit_off + i), u1 = __ldg(M.unit_off + i + 1);
             for (int u = u0; u < u1; ++u) v += sm->part[u];
         }
-        out[s] = v;
+        out.v[s] = v;
     }
     __syncwarp();
+    return out;
 }
 
 // f = dy/dt for the warp's cell.  y, f: lane elements in internal order.
@@ -333,14 +364,20 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
     for (int s = 0; s < MT::NS; ++s) y[s] = yv.v[s];
     double Yk[MT::NS], cpR[MT::NS], hRT[MT::NS], dcpR[MT::NS];
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
+    const RxnCtx rc = rxn_ctx(c);
+    const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        sm->q[s] = rxn_eval<false>(M, MT::ID, s, c, sm->C, sm->G).q;
+        sm->q[s] = rxn_slot(MT::ID, s, rc, C_off, G_off, 0).q;
     }
     __syncwarp();
     double om[MT::NS];
-    gather<MT>(M, sm->q, sm, lane, om);
+    {
+        const Vec<MT::NS> g = gather<MT, false>(nullptr, smem_off(sm->q), chem_off, lane);
+#pragma unroll
+        for (int s = 0; s < MT::NS; ++s) om[s] = g.v[s];
+    }
     double qsum = 0.0, cpsum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
@@ -385,10 +422,12 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
     const int ns = M.nslot;
+    const RxnCtx rc = rxn_ctx(c);
+    const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        const RxnOut o = rxn_eval<true>(M, MT::ID, s, c, sm->C, sm->G);
+        const RxnOut o = rxn_slot(MT::ID, s, rc, C_off, G_off, 1);
         const int fl = __ldg(M.flags + s);
         double dqdT = 0.0, sr = 0.0, thd_term = 0.0;
         double dRf[3] = {0.0, 0.0, 0.0}, dRr[3] = {0.0, 0.0, 0.0};
@@ -460,12 +499,16 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     }
     __syncwarp();
     // per-species totals (fixed-order gathers)
-    double w[NS], dw[NS], sk[NS];
-    gather<MT>(M, sm->q, sm, lane, w);
-    gather<MT>(M, js->dqdT, sm, lane, dw);
-    gather<MT>(M, js->sr, sm, lane, sk);
+    const Vec<NS> wv = gather<MT, false>(nullptr, smem_off(sm->q), chem_off, lane);
+    const Vec<NS> dwv = gather<MT, true>(js->dqdT, 0u, chem_off, lane);
+    const Vec<NS> skv = gather<MT, true>(js->sr, 0u, chem_off, lane);
+    const double (&w)[NS] = wv.v;
+    const double (&dw)[NS] = dwv.v;
+    const double (&sk)[NS] = skv.v;
     double* spw = sm->q;   // per-species work reuses the rate buffer: [3][N]
-    const double WN = __ldg(M.mw + N - 1);
+    const double inv_rho = 1.0 / c.rho;
+    const double iWN = __ldg(M.inv_mw + N - 1);
+    const double RT = kRU * c.T;
     double dfdT[NS];
     double qsum = 0.0, cpsum = 0.0, Ssum2 = 0.0, Ssum3 = 0.0, accTT = 0.0, dcpsum = 0.0;
 #pragma unroll
@@ -473,28 +516,30 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
         const int i = lane + 32 * s;
         dfdT[s] = 0.0;
         if (i < N) {
-            const double Wi = __ldg(M.mw + i);
-            const double fk = w[s] * Wi / c.rho;
-            dfdT[s] = (Wi / c.rho) * (dw[s] + w[s] * c.invT);
-            const double hk = kRU * c.T * hRT[s] / Wi;     // J/kg
-            const double cpk = kRU * cpR[s] / Wi;          // J/kg/K
-            const double X = (c.mw_avg / c.rho) * (w[s] - sk[s]);
-            spw[0 * N + i] = hk * Wi;                      // h_k W_k
+            const double Wi = __ldg(M.mw + i), iWi = __ldg(M.inv_mw + i);
+            const double Wr = Wi * inv_rho;
+            const double fk = w[s] * Wr;
+            dfdT[s] = Wr * (dw[s] + w[s] * c.invT);
+            const double hW = RT * hRT[s];                 // h_k W_k  [J/kmol]
+            const double hk = hW * iWi;                    // J/kg
+            const double cpk = kRU * cpR[s] * iWi;         // J/kg/K
+            const double X = (c.mw_avg * inv_rho) * (w[s] - sk[s]);
+            spw[0 * N + i] = hW;
             spw[1 * N + i] = cpk;
             spw[2 * N + i] = X;
             qsum += hk * fk;
             cpsum += cpk * Yk[s];
-            Ssum2 += hk * Wi * (double)A[i * LDA + (N - 1)];
-            Ssum3 += hk * Wi * X;
+            Ssum2 += hW * (double)A[i * LDA + (N - 1)];
+            Ssum3 += hW * X;
             accTT += cpk * fk + hk * dfdT[s];
-            dcpsum += Yk[s] * kRU * dcpR[s] / Wi;
+            dcpsum += Yk[s] * kRU * dcpR[s] * iWi;
         }
     }
-    const double cp_avg = warp_sum(cpsum);
-    const double fT = -warp_sum(qsum) / cp_avg;
+    const double inv_cp = 1.0 / warp_sum(cpsum);
+    const double fT = -warp_sum(qsum) * inv_cp;
     const double S2 = warp_sum(Ssum2);
     const double S3 = warp_sum(Ssum3);
-    const double JTT = -(warp_sum(accTT) + fT * warp_sum(dcpsum)) / cp_avg;
+    const double JTT = -(warp_sum(accTT) + fT * warp_sum(dcpsum)) * inv_cp;
     __syncwarp();
     // T row (state row N-1): lane owns columns j < N-1
     double trow[NS];
@@ -504,11 +549,10 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
         trow[s] = 0.0;
         if (j < N - 1) {
             double S1 = 0.0;
-#pragma unroll 4
+#pragma unroll 1
             for (int k = 0; k < N; ++k) S1 += spw[k] * (double)A[k * LDA + j];
-            const double Wj = __ldg(M.mw + j);
-            const double dj = 1.0 / Wj - 1.0 / WN;
-            trow[s] = -(S1 / Wj - S2 / WN + dj * S3 + fT * (spw[N + j] - spw[N + N - 1])) / cp_avg;
+            const double iWj = __ldg(M.inv_mw + j);
+            trow[s] = -(S1 * iWj - S2 * iWN + (iWj - iWN) * S3 + fT * (spw[N + j] - spw[N + N - 1])) * inv_cp;
         }
     }
     __syncwarp();
@@ -519,12 +563,12 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
         if (k < N - 1) {
             LinT* row = A + k * LDA;
             const double Wk = __ldg(M.mw + k);
-            const double cN = (double)row[N - 1] / WN;
+            const double cN = (double)row[N - 1] * iWN;
             const double X = spw[2 * N + k];
-#pragma unroll 4
+#pragma unroll 1
             for (int j = 0; j < N - 1; ++j) {
                 const double iWj = __ldg(M.inv_mw + j);
-                row[j] = (LinT)(Wk * ((double)row[j] * iWj - cN + X * (iWj - 1.0 / WN)));
+                row[j] = (LinT)(Wk * ((double)row[j] * iWj - cN + X * (iWj - iWN)));
             }
             row[N - 1] = (LinT)dfdT[s];
         }
