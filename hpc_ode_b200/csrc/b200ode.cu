@@ -282,10 +282,37 @@ b200ode_status ensure_wg(b200ode_handle* h, size_t bytes) {
     return B200ODE_OK;
 }
 
+// Warps per CTA: the option when set, else the shape (4, 2 or 1 warps per CTA)
+// that keeps the most warps resident per SM for this mechanism and precision
+// (shared memory per warp and registers decide), ties to the larger CTA.
+// Computed once per handle.
+template <class MT, class LinT>
+int pick_wpb(b200ode_handle* h) {
+    if (h->opt.warps_per_block > 0) return std::min(h->opt.warps_per_block, 4);
+    if (h->auto_wpb > 0) return h->auto_wpb;
+    int best = 4, best_warps = -1;
+    for (int wpb : {4, 2, 1}) {
+        const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+        auto k = k_bdf<MT, LinT, 1>;
+        int bps = 0;
+        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, wpb * 32, smem) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        if (bps * wpb > best_warps) {
+            best_warps = bps * wpb;
+            best = wpb;
+        }
+    }
+    h->auto_wpb = best;
+    return best;
+}
+
 template <class MT, class LinT>
 b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
     using R = StepRecord<MT, LinT>;
-    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
     auto kern = k_bdf<MT, LinT, 1>;
     if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
@@ -381,7 +408,7 @@ b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
 template <class MT, class LinT>
 b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KParams), long long* blocks,
                                 int* wpb_out, size_t* smem_out) {
-    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
     auto k = k_bdf<MT, LinT, 1>;
     if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) k = k_bdf<MT, LinT, 3>;
@@ -799,6 +826,71 @@ b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n, const double*
     return eval_chem(h, n, P, Ps, T, Y, nullptr, nullptr, jac);
 }
 
+b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, double Ps, const double* dT,
+                                const double* dY, double t0, double t1, int32_t* wpb_out, int32_t* bps_out) {
+    b200ode_status rc = check_args(h, n, t0, t1);
+    if (rc != B200ODE_OK) return rc;
+    if (n <= 0 || !dT || !dY) return fail(B200ODE_ERR_INVALID, "autotune needs cells (device T and Y)");
+    if (!dP && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
+    const int64_t m = std::min<int64_t>(n, 8192);
+    const size_t nsp = h->hm.nsp;
+    rc = ensure_cap(h, (size_t)m);
+    if (rc != B200ODE_OK) return rc;
+    cudaStream_t st = h->stream;
+    // the sample: the first m cells, copied so the caller's buffers stay untouched
+    double *sT = nullptr, *sY = nullptr;
+    CUDA_TRY(cudaMallocAsync(&sT, m * sizeof(double), st));
+    CUDA_TRY(cudaMallocAsync(&sY, m * nsp * sizeof(double), st));
+    CUDA_TRY(cudaMemcpyAsync(sT, dT, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    CUDA_TRY(cudaMemcpy2DAsync(sY, m * sizeof(double), dY, n * sizeof(double), m * sizeof(double), nsp,
+                               cudaMemcpyDeviceToDevice, st));
+    if (dP) CUDA_TRY(cudaMemcpyAsync(h->d_P, dP, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    const b200ode_options saved = h->opt;
+    // warps per CTA x register variant (blocks_per_sm >= 3 * 4 / wpb selects the
+    // 168-register variant, which trades spills for resident warps)
+    const int cand[6][2] = {{4, 0}, {2, 0}, {1, 0}, {4, 3}, {2, 6}, {1, 12}};
+    float best_ms = 0.f;
+    int best = -1;
+    h->opt.persistent = 1;
+    for (int c = 0; c < 6 && rc == B200ODE_OK; ++c) {
+        h->opt.warps_per_block = cand[c][0];
+        h->opt.blocks_per_sm = cand[c][1];
+        float ms_c = 1e30f;
+        for (int rep = 0; rep < 2 && rc == B200ODE_OK; ++rep) {
+            if (cudaMemcpyAsync(h->d_T, sT, m * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+                cudaMemcpyAsync(h->d_Y, sY, m * nsp * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
+                rc = fail(B200ODE_ERR_CUDA, "autotune: sample copy");
+                break;
+            }
+            KParams p;
+            fill_params(h, p, m, dP ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, h->d_status, nullptr, t0, t1);
+            int launches = 0;
+            if (cudaEventRecord(h->ev[1], st) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "event"); break; }
+            rc = run(h, p, st, &launches);
+            if (rc != B200ODE_OK) break;
+            cudaEventRecord(h->ev[2], st);
+            if (cudaEventSynchronize(h->ev[2]) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "autotune run"); break; }
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+            ms_c = std::min(ms_c, ms);
+        }
+        if (rc == B200ODE_OK && (best < 0 || ms_c < best_ms)) {
+            best_ms = ms_c;
+            best = c;
+        }
+    }
+    cudaFreeAsync(sT, st);
+    cudaFreeAsync(sY, st);
+    cudaStreamSynchronize(st);
+    h->opt = saved;
+    if (rc != B200ODE_OK) return rc;
+    h->opt.warps_per_block = cand[best][0];
+    h->opt.blocks_per_sm = cand[best][1];
+    if (wpb_out) *wpb_out = cand[best][0];
+    if (bps_out) *bps_out = cand[best][1];
+    return B200ODE_OK;
+}
+
 b200ode_status b200ode_fp64_peak(int32_t device, double* gflops) {
     if (!gflops) return fail(B200ODE_ERR_INVALID, "null output");
     if (device >= 0) CUDA_TRY(cudaSetDevice(device));
@@ -894,7 +986,7 @@ template <class MT, class LinT>
 b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* scratch, cudaStream_t st,
                                   int* launches) {
     using WG = WarpGlobal<MT, LinT>;
-    const int wpb = h->opt.warps_per_block > 0 ? std::min(h->opt.warps_per_block, 4) : 4;
+    const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
     auto kern = k_bdf<MT, LinT, 1>;
     if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;

@@ -33,6 +33,7 @@ struct b200ode_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int last_blocks_per_sm = 0;
+    int auto_wpb = 0;                        // warps per CTA picked by occupancy (0 = not yet)
 };
 
 namespace b200 {

@@ -96,12 +96,15 @@ __device__ __forceinline__ WarpSmem<MT, LinT>* wsm(unsigned off) {
 template <int NS>
 __device__ __forceinline__ bool valid_el(int lane, int s, int N) { return lane + 32 * s < N; }
 
+// sqrt(sum over the warp of acc / n): the tail of every WRMS norm, out of line.
+__device__ __noinline__ double wrms_reduce(double acc, int n) { return sqrt(warp_sum(acc) / n); }
+
 template <int NS>
 __device__ __forceinline__ double wrms_v(const double (&x)[NS], const double (&w)[NS], int N) {
     double acc = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) { const double t = x[s] * w[s]; acc += t * t; }
-    return sqrt(warp_sum(acc) / N);
+    return wrms_reduce(acc, N);
 }
 
 template <class MT, class LinT>
@@ -109,7 +112,7 @@ __device__ __forceinline__ double wrms_zn(const WarpSmem<MT, LinT>* w, int j, co
     double acc = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) { const double t = w->zn[j][lane + 32 * s] * ewt[s]; acc += t * t; }
-    return sqrt(warp_sum(acc) / MT::N);
+    return wrms_reduce(acc, MT::N);
 }
 
 __device__ __forceinline__ long long ph_tick(const BdfState& S) { return S.profiling ? clock64() : 0; }
@@ -510,7 +513,7 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
         z0[s] = valid_el<NS>(lane, s, N) ? y0.v[s] : 0.0;
-        ewt[s] = valid_el<NS>(lane, s, N) ? 1.0 / (S.rtol * fabs(z0[s]) + S.atol) : 0.0;
+        ewt[s] = valid_el<NS>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(z0[s]) + S.atol) : 0.0;
     }
     bdf_rhs<MT, LinT>(off, z0, z1, lane);
 #pragma unroll
@@ -608,7 +611,7 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
         // ---- CVode loop: error weights, work limit, accuracy check
 #pragma unroll
         for (int s = 0; s < NS; ++s)
-            ewt[s] = valid_el<NS>(lane, s, N) ? 1.0 / (S.rtol * fabs(w->zn[0][lane + 32 * s]) + S.atol) : 0.0;
+            ewt[s] = valid_el<NS>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(w->zn[0][lane + 32 * s]) + S.atol) : 0.0;
         if (S.nstloc >= S.max_steps) { done = true; return cv::CV_TOO_MUCH_WORK; }
         if (cv::UROUND * wrms_zn<MT, LinT>(w, 0, ewt, lane) > 1.0) { done = true; return cv::CV_TOO_MUCH_ACC; }
         // ---- cvStep

@@ -118,6 +118,18 @@ struct CellThermo {
     double T, logT, invT, m, rho, mw_avg, yN, mC;   // mC = m - sum_k C_k
 };
 
+// Out-of-line FP64 transcendentals: one copy of each library routine in the
+// kernel image instead of one per call site.  The integration kernel is bound
+// by instruction fetch (its hot code is larger than the SM's instruction
+// cache), so every call site that is not a full inline expansion helps.
+__device__ __noinline__ double ode_exp(double x) { return exp(x); }
+__device__ __noinline__ double ode_log10(double x) { return log10(x); }
+__device__ __noinline__ double ode_exp10(double x) { return exp10(x); }
+__device__ __noinline__ double ode_pow(double x, double y) { return pow(x, y); }
+// IEEE division out of line: an inline FP64 division is ~40 instructions, so
+// the scalar step-control code calls this single copy instead.
+__device__ __noinline__ double ode_div(double a, double b) { return a / b; }
+
 // Species phase: concentrations and Gibbs terms into shared memory.
 template <class MT>
 __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, const double (&y)[MT::NS],
@@ -141,11 +153,11 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
         Yk[s] = (i < N - 1) ? y[s] : ((i == N - 1) ? c.yN : 0.0);
         if (i < N) sw += Yk[s] * __ldg(M.inv_mw + i);
     }
-    c.mw_avg = 1.0 / warp_sum(sw);
+    c.mw_avg = ode_div(1.0, warp_sum(sw));
     c.logT = log(c.T);
-    c.invT = 1.0 / c.T;
-    c.rho = P * c.mw_avg / (kRU * c.T);
-    c.m = P / (kRU * c.T);
+    c.invT = ode_div(1.0, c.T);
+    c.rho = ode_div(P * c.mw_avg, kRU * c.T);
+    c.m = ode_div(P, kRU * c.T);
     double csum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
@@ -172,17 +184,6 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     return c;
 }
 
-// Out-of-line FP64 transcendentals: one copy of each library routine in the
-// kernel image instead of one per call site.  The integration kernel is bound
-// by instruction fetch (its hot code is larger than the SM's instruction
-// cache), so every call site that is not a full inline expansion helps.
-__device__ __noinline__ double ode_exp(double x) { return exp(x); }
-__device__ __noinline__ double ode_log10(double x) { return log10(x); }
-__device__ __noinline__ double ode_exp10(double x) { return exp10(x); }
-__device__ __noinline__ double ode_pow(double x, double y) { return pow(x, y); }
-// IEEE division out of line: an inline FP64 division is ~40 instructions, so
-// the scalar step-control code calls this single copy instead.
-__device__ __noinline__ double ode_div(double a, double b) { return a / b; }
 
 // Rates of one reaction slot.  With Deriv, also the pieces of its derivative.
 struct RxnOut {
@@ -389,12 +390,13 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
     }
     const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k h_k W_k   [W/m^3]
     const double cp_avg = kRU * warp_sum(cpsum);           // [J/kg/K]
-    const double dTdt = -Q / (c.rho * cp_avg);
+    const double dTdt = ode_div(-Q, c.rho * cp_avg);
+    const double inv_rho = ode_div(1.0, c.rho);
     Vec<MT::NS> fv;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
         const int i = lane + 32 * s;
-        if (i < N - 1) fv.v[s] = om[s] * (__ldg(M.mw + i) / c.rho);
+        if (i < N - 1) fv.v[s] = om[s] * (__ldg(M.mw + i) * inv_rho);
         else if (i == N - 1) fv.v[s] = dTdt;
         else fv.v[s] = 0.0;
     }
@@ -506,7 +508,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     const double (&dw)[NS] = dwv.v;
     const double (&sk)[NS] = skv.v;
     double* spw = sm->q;   // per-species work reuses the rate buffer: [3][N]
-    const double inv_rho = 1.0 / c.rho;
+    const double inv_rho = ode_div(1.0, c.rho);
     const double iWN = __ldg(M.inv_mw + N - 1);
     const double RT = kRU * c.T;
     double dfdT[NS];
@@ -535,7 +537,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             dcpsum += Yk[s] * kRU * dcpR[s] * iWi;
         }
     }
-    const double inv_cp = 1.0 / warp_sum(cpsum);
+    const double inv_cp = ode_div(1.0, warp_sum(cpsum));
     const double fT = -warp_sum(qsum) * inv_cp;
     const double S2 = warp_sum(Ssum2);
     const double S3 = warp_sum(Ssum3);

@@ -27,7 +27,7 @@ EXPORTED = ["b200ode_default_options", "b200ode_create", "b200ode_destroy", "b20
             "b200ode_mechanism_species",
             "b200ode_integrate", "b200ode_integrate_device", "b200ode_integrate_device_noalloc",
             "b200ode_eval_rhs",
-            "b200ode_eval_jacobian", "b200ode_fp64_peak",
+            "b200ode_eval_jacobian", "b200ode_autotune", "b200ode_fp64_peak",
             "b200ode_default_server_options", "b200ode_server_create", "b200ode_server_destroy",
             "b200ode_submit", "b200ode_poll", "b200ode_server_get_report",
             "b200ode_last_error", "b200ode_version"]
@@ -119,6 +119,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.b200ode_eval_rhs.restype = C.c_int
     lib.b200ode_eval_jacobian.argtypes = [C.c_void_p, C.c_int64, _dp, C.c_double, _dp, _dp, _dp]
     lib.b200ode_eval_jacobian.restype = C.c_int
+    lib.b200ode_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                     C.c_double, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    lib.b200ode_autotune.restype = C.c_int
     lib.b200ode_fp64_peak.argtypes = [C.c_int32, C.POINTER(C.c_double)]
     lib.b200ode_fp64_peak.restype = C.c_int
     lib.b200ode_default_server_options.argtypes = [C.POINTER(ServerOptions)]
@@ -243,6 +246,16 @@ class Solver:
             C.byref(st) if st is not None else None, C.c_void_p(stream or None)))
         self.last_stats = st
         return stats_dict(st) if st is not None else None
+
+    def autotune(self, n: int, dP: int, P_scalar: float, dT: int, dY: int, t1: float, t0: float = 0.0):
+        """Pick the fastest launch shape on a sample of these device-resident
+        cells (left unmodified); later calls on this solver use it.  Returns
+        (warps per CTA, blocks-per-SM setting)."""
+        w, b = C.c_int32(), C.c_int32()
+        _check(self.lib.b200ode_autotune(self.h, n, C.c_void_p(dP or None), float(P_scalar), C.c_void_p(dT),
+                                         C.c_void_p(dY), float(t0), float(t1), C.byref(w), C.byref(b)))
+        self.opts.warps_per_block, self.opts.blocks_per_sm = w.value, b.value
+        return w.value, b.value
 
     def integrate_device_noalloc(self, n: int, dP: int, P_scalar: float, dT: int, dY: int, t1: float,
                                  t0: float = 0.0, dstatus: int = 0, stream: int = 0, want_stats=True):

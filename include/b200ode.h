@@ -186,6 +186,18 @@ b200ode_status b200ode_eval_rhs(b200ode_handle* h, int64_t n_cells, const double
 b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n_cells, const double* P,
                                      double P_scalar, const double* T, const double* Y, double* jac);
 
+/* Autotuner: integrates a sample of the given cells (the first min(n_cells,
+ * 8192); device buffers as b200ode_integrate_device, left unmodified) with the
+ * persistent kernel under each launch shape -- 4, 2 or 1 warps (cells) per CTA,
+ * each with the full-register or the 168-register kernel variant -- and keeps
+ * the fastest in the handle's options (warps_per_block, blocks_per_sm), which
+ * later calls on this handle use.  The chosen values are also returned (either
+ * pointer may be NULL).  Results of an integration do not depend on the launch
+ * shape.  No reference counterpart (the reference has no tunable kernels). */
+b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n_cells, const double* d_P, double P_scalar,
+                                const double* d_T, const double* d_Y, double t0, double t1,
+                                int32_t* warps_per_block, int32_t* blocks_per_sm);
+
 /* Diagnostic: measured FP64 FMA throughput of a device (GFLOP/s), the
  * denominator of the FP64-pipe roofline this library reports.  No reference
  * counterpart (a measurement helper). */

@@ -1,0 +1,34 @@
+"""The launch-shape autotuner (b200ode_autotune): it leaves the sample cells
+untouched, picks one of its candidate shapes, and integration results do not
+depend on the launch shape (bitwise)."""
+import numpy as np
+import pytest
+
+from hpc_ode_b200 import native, workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("precision", [native.B200ODE_MIXED, native.B200ODE_FP64])
+def test_autotune_picks_a_shape_and_results_do_not_change(precision):
+    import torch
+    b = W.make("gri_32k", 3000, seed=17)
+    T = torch.from_numpy(b.T.copy()).cuda()
+    Y = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
+    P = torch.from_numpy(b.P.copy()).cuda()
+    T0, Y0 = T.clone(), Y.clone()
+    s = native.Solver("gri30", precision=precision)
+    wpb, bps = s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+    torch.cuda.synchronize()
+    assert (wpb, bps) in {(4, 0), (2, 0), (1, 0), (4, 3), (2, 6), (1, 12)}
+    assert torch.equal(T, T0) and torch.equal(Y, Y0)          # sample left untouched
+    st = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
+    s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt, dstatus=st.data_ptr())
+    s.close()
+    ref = native.Solver("gri30", precision=precision, warps_per_block=4)
+    T2, Y2 = T0.clone(), Y0.clone()
+    ref.integrate_device(b.ncells, P.data_ptr(), 0.0, T2.data_ptr(), Y2.data_ptr(), b.dt)
+    ref.close()
+    torch.cuda.synchronize()
+    assert (st == 0).all()
+    assert torch.equal(T, T2) and torch.equal(Y, Y2)

@@ -10,9 +10,11 @@ in mixed mode):
     differences of the reference RHS instead); FP32 form (FP32 accumulation): 1e-4;
   * integration vs the CPU oracle at the same tolerances (rtol 1e-6, atol
     1e-10): |dT|/T <= 1e-5 for every cell; per species |dY| <= max(1e-4 |Y|,
-    1e-10) for at least 99 % of entries, the rest within the integration error
-    of a rtol-1e-6 CVODE integration (the CPU integrator itself misses that gate
-    against a rtol-1e-10 solution for 0.5-5 % of entries).
+    1e-10) for at least 99 % of entries (batches of 500+ entries), and every
+    entry that misses it within the integration error of a rtol-1e-6 CVODE
+    integration: |Y - Y_true| <= 10 (|Y_cpu - Y_true| + rtol |Y_true| + atol)
+    against the FP64 oracle at rtol 1e-10 (the CPU integrator itself misses the
+    per-entry gate against that solution for 2-4 % of entries).
 """
 import numpy as np
 import pytest
@@ -34,11 +36,24 @@ def run_gpu(b, precision, persistent=1, use_graph=0, counters=False, **kw):
     return T, Y, st, stats, cnt
 
 
-def compare(b, T, Y, yo, label):
+def compare(b, T, Y, yo, label, oracle=None):
     dT = np.abs(T - yo[:, 0]) / yo[:, 0]
-    ok = y_ok(Y[:-1].T, yo[:, 1:])
+    Yg = Y[:-1].T
+    ok = y_ok(Yg, yo[:, 1:])
     assert dT.max() <= GATE_T, (label, dT.max())
-    assert ok.mean() >= 0.99, (label, ok.mean())
+    if ok.size >= 500:
+        assert ok.mean() >= 0.99, (label, ok.mean())
+    if not ok.all():
+        assert oracle is not None, (label, "entries outside the gate and no oracle to bound them")
+        cells = np.nonzero(~ok.all(axis=1))[0]
+        sub = b.subset(cells)
+        yt, st = oracle.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=1e-10, atol=1e-14, threads=8)
+        assert (st["status"] == 0).all()
+        true = yt[:, 1:]
+        bound = 10.0 * (np.abs(yo[cells, 1:] - true) + W.RTOL * np.abs(true) + W.ATOL)
+        miss = ~ok[cells]
+        err = np.abs(Yg[cells] - true)
+        assert (err[miss] <= bound[miss]).all(), (label, float((err[miss] / bound[miss]).max()))
     return dT, ok
 
 
@@ -87,7 +102,7 @@ def test_integration_matches_oracle(oracle, wl, n, precision):
     yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, rtol=W.RTOL, atol=W.ATOL, threads=8)
     T, Y, st, stats, cnt = run_gpu(b, precision, counters=True)
     assert (st == 0).all() and (so["status"] == 0).all()
-    compare(b, T, Y, yo, f"{wl}/{precision}")
+    compare(b, T, Y, yo, f"{wl}/{precision}", oracle)
     # mass conservation of the returned state (closure species)
     assert np.abs(Y.sum(axis=0) - 1.0).max() < 1e-12
     # step and Newton counts track the oracle's (same algorithm)
@@ -125,7 +140,7 @@ def test_ragged_batch_sizes(oracle, n):
     yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, threads=8)
     T, Y, st, _, _ = run_gpu(b, native.B200ODE_MIXED)
     assert (st == 0).all()
-    compare(b, T, Y, yo, f"n={n}")
+    compare(b, T, Y, yo, f"n={n}", oracle)
 
 
 def test_h2_1025_cells_fp64(oracle):
@@ -133,7 +148,7 @@ def test_h2_1025_cells_fp64(oracle):
     yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, threads=8)
     T, Y, st, _, _ = run_gpu(b, native.B200ODE_FP64)
     assert (st == 0).all()
-    compare(b, T, Y, yo, "h2 1025")
+    compare(b, T, Y, yo, "h2 1025", oracle)
 
 
 def test_quiescent_reference_e2e(golden_e2e):
