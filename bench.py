@@ -180,6 +180,62 @@ def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample
             "oracle_failed": int((st_true["status"] != 0).sum())}
 
 
+def serving_block(native, device: int, n_requests: int, load: float, seed: int = 4) -> dict:
+    """Serving loop under Poisson arrivals: requests of the serving workload
+    (log-uniform 1k-256k cells, 60 % H2 / 40 % GRI, dt in {1e-5, 1e-4}) are
+    submitted at exponential inter-arrival times with rate load x the measured
+    saturation request rate; latency is submit -> results in the caller's host
+    buffers (measured by the library's dispatcher thread)."""
+    cal = list(W.serving_requests(12, seed=seed + 1))
+    reqs = list(W.serving_requests(n_requests, seed=seed))
+    srv = native.Server(max_inflight=4, device=device)
+    try:
+        # saturation: the calibration requests submitted at once (also warms handles and staging)
+        t0 = time.perf_counter()
+        ids = [srv.submit(b.mech, b.T.copy(), np.ascontiguousarray(b.Y.copy()), b.P, b.dt) for b in cal]
+        for r in ids:
+            srv.poll(r, -1)
+        sat = len(cal) / (time.perf_counter() - t0)
+        rate = load * sat
+        rng = np.random.default_rng(seed + 7)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+        bufs = [(b.T.copy(), np.ascontiguousarray(b.Y.copy())) for b in reqs]
+        pending, infos = [], []
+        start = time.perf_counter()
+        for b, (T, Y), ta in zip(reqs, bufs, arrivals):
+            while True:
+                now = time.perf_counter() - start
+                pending = [r for r in pending if not _take(srv, r, infos)]
+                if now >= ta:
+                    break
+                time.sleep(min(0.002, ta - now))
+            pending.append(srv.submit(b.mech, T, Y, b.P, b.dt))
+        for r in pending:
+            st, info = srv.poll(r, -1)
+            infos.append(info)
+        span = time.perf_counter() - start
+        lat = np.array([i["latency_ms"] for i in infos])
+        cells = int(sum(i["n_cells"] for i in infos))
+        rep = srv.report()
+        return {"requests": len(infos), "offered_load": load, "saturation_req_per_s": sat,
+                "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+                "max_latency_ms": float(lat.max()), "mean_queue_ms": float(np.mean([i["queue_ms"] for i in infos])),
+                "cells_per_sec": cells / span, "cells": cells, "max_concurrent": rep["max_concurrent"],
+                "failed_cells": int(sum(i["n_failed"] for i in infos)),
+                "workload": "log-uniform 1k-256k cells, 60 % H2 (h2_1024 dists) / 40 % GRI (gri_32k dists), "
+                            "dt in {1e-5, 1e-4} s, Poisson arrivals, host buffers"}
+    finally:
+        srv.close()
+
+
+def _take(srv, rid, infos) -> bool:
+    r = srv.poll(rid, 0)
+    if r is None:
+        return False
+    infos.append(r[1])
+    return True
+
+
 def fp64_peak_gflops(torch, native_mod) -> float:
     """Measured FP64 FMA throughput of this GPU (library microkernel), GFLOP/s."""
     try:
@@ -203,6 +259,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-fp64-step", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serving-requests", type=int, default=48)
+    ap.add_argument("--serving-load", type=float, default=0.8)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -341,6 +401,39 @@ def main():
     except Exception as e:  # noqa: BLE001
         fp64 = {"error": str(e)}
 
+    # ---- the plain FP64 one-launch-per-step form on the same cells (the
+    # comparison the mixed persistent form is measured against)
+    fp64_step = None
+    if not args.no_fp64_step and args.precision == "mixed" and args.form == "persistent":
+        ref = native.Solver(batch.mech, precision=native.B200ODE_FP64, persistent=0, device=dev.index)
+        Ts, Ys = torch.empty_like(T0), torch.empty_like(Y0)
+        times = []
+        for k in range(2):
+            Ts.copy_(T0)
+            Ys.copy_(Y0)
+            flush.zero_()
+            torch.cuda.synchronize(dev)
+            a = torch.cuda.Event(enable_timing=True)
+            bev = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ref.integrate_device(n, P.data_ptr(), 0.0, Ts.data_ptr(), Ys.data_ptr(), batch.dt,
+                                 stream=stream.cuda_stream, want_stats=False)
+            bev.record(stream)
+            torch.cuda.synchronize(dev)
+            times.append(a.elapsed_time(bev))
+        ref.close()
+        fp64_ms = times[-1]
+        fp64_step = {"value": n / (fp64_ms * 1e-3), "unit": "cells/s", "ms_per_step": fp64_ms,
+                     "form": "FP64 Newton matrix, one launch per BDF step, state in HBM between launches",
+                     "steps": "1 warm-up + 1 timed", "mixed_persistent_speedup": fp64_ms / kernel_ms}
+
+    serving = None
+    if rank == 0 and not args.no_serving:
+        try:
+            serving = serving_block(native, dev.index, args.serving_requests, args.serving_load)
+        except Exception as e:  # noqa: BLE001
+            serving = {"error": str(e)}
+
     acc = None
     if rank == 0 and not args.no_accuracy:
         try:
@@ -374,6 +467,8 @@ def main():
         "roofline": roofline,
         "fp64": fp64,
         "cpu_baseline": cpu,
+        "fp64_step_form": fp64_step,
+        "serving": serving,
         "accuracy": acc,
         "clocks": clk,
     }

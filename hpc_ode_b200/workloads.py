@@ -122,3 +122,21 @@ WORKLOADS = {
                    phi=(0.4, 2.5), P_atm=(1.0, 40.0)),
 }
 RTOL, ATOL = 1e-6, 1e-10
+
+
+def serving_requests(n_requests: int, seed: int = 4, min_cells: int = 1024, max_cells: int = 262144):
+    """The serving workload: requests of log-uniform size in [min_cells,
+    max_cells], drawn 60 % from the H2 distributions (h2_1024) and 40 % from the
+    GRI distributions (gri_32k), each with dt uniform in {1e-5, 1e-4} s.
+    Deterministic for a seed; yields Batch objects."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(min_cells), np.log(max_cells)
+    for i in range(n_requests):
+        n = int(np.exp(rng.uniform(lo, hi)))
+        wl = "h2_1024" if rng.random() < 0.6 else "gri_32k"
+        dt = float(rng.choice([1e-5, 1e-4]))
+        b = make(wl, n, seed=seed * 1_000_003 + i)
+        b.dt = dt
+        b.name = f"serve[{i}]:{wl}:{n}:{dt:g}"
+        yield b
+
