@@ -200,9 +200,10 @@ struct FallOut {
     double phi, dphi_dthd, dphi_dT;
 };
 
-__device__ __noinline__ FallOut falloff(int mech_id, int s, int fl, double T, double logT, double invT,
+template <class MT>
+__device__ __noinline__ FallOut falloff(int s, int fl, double T, double logT, double invT,
                                         double kf, double thd, int Deriv) {
-    const DevMech& M = c_mech[mech_id];
+    const DevMech& M = mech<MT>();
     const int type = fl & kFlagTypeMask;
     struct { double T, logT, invT; } c = {T, logT, invT};
     FallOut o;
@@ -261,11 +262,13 @@ struct RxnCtx {
 
 // Rates of reaction slot s; with deriv, also the pieces of its derivative.
 // Out of line and shared by the RHS and the Jacobian: one copy of the reaction
-// code in the instruction cache.  C_off / G_off: shared-memory byte offsets of
-// the concentrations and -g/RT (index N holds the padding entries).
-__device__ __noinline__ RxnOut rxn_slot(int mech_id, int s, const RxnCtx c, unsigned C_off, unsigned G_off,
-                                        int deriv) {
-    const DevMech& M = c_mech[mech_id];
+// code in the instruction cache (a separate q-only copy for the RHS measured
+// slower: the kernel is bound by instruction fetch).  C_off / G_off:
+// shared-memory byte offsets of the concentrations and -g/RT (index N holds the
+// padding entries).
+template <class MT>
+__device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, unsigned G_off, int deriv) {
+    const DevMech& M = mech<MT>();
     const double* C = smem_at<double>(C_off);
     const double* G = smem_at<double>(G_off);
     RxnOut o;
@@ -273,7 +276,7 @@ __device__ __noinline__ RxnOut rxn_slot(int mech_id, int s, const RxnCtx c, unsi
     o.dphi_dthd = 0.0; o.dphi_dT = 0.0; o.dlnkf_dT = 0.0;
     const int fl = __ldg(M.flags + s);
     if (!(fl & kFlagActive)) return o;
-    const int ns = M.nslot;
+    constexpr int ns = MT::NSLOT;
     const int r0 = __ldg(M.rf + s), r1 = __ldg(M.rf + ns + s), r2 = __ldg(M.rf + 2 * ns + s);
     const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
     const double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
@@ -306,7 +309,7 @@ __device__ __noinline__ RxnOut rxn_slot(int mech_id, int s, const RxnCtx c, unsi
             o.phi = thd;
             o.dphi_dthd = 1.0;
         } else {
-            const FallOut f = falloff(mech_id, s, fl, c.T, c.logT, c.invT, kf, thd, deriv);
+            const FallOut f = falloff<MT>(s, fl, c.T, c.logT, c.invT, kf, thd, deriv);
             o.phi = f.phi;
             o.dphi_dthd = f.dphi_dthd;
             o.dphi_dT = f.dphi_dT;
@@ -370,7 +373,7 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        sm->q[s] = rxn_slot(MT::ID, s, rc, C_off, G_off, 0).q;
+        sm->q[s] = rxn_slot<MT>(s, rc, C_off, G_off, 0).q;
     }
     __syncwarp();
     double om[MT::NS];
@@ -423,13 +426,13 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
 #pragma unroll 2
     for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
-    const int ns = M.nslot;
+    constexpr int ns = MT::NSLOT;
     const RxnCtx rc = rxn_ctx(c);
     const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
         const int s = 32 * g + lane;
-        const RxnOut o = rxn_slot(MT::ID, s, rc, C_off, G_off, 1);
+        const RxnOut o = rxn_slot<MT>(s, rc, C_off, G_off, 1);
         const int fl = __ldg(M.flags + s);
         double dqdT = 0.0, sr = 0.0, thd_term = 0.0;
         double dRf[3] = {0.0, 0.0, 0.0}, dRr[3] = {0.0, 0.0, 0.0};
