@@ -25,6 +25,7 @@
 #include "bdf_warp.cuh"
 #include "mech/gri30_mech.h"
 #include "mech/h2o2_mech.h"
+#include "mech/nDodecane_Reitz_mech.h"
 
 using namespace b200;
 
@@ -54,10 +55,11 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
               tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp,  \
               tag##_tb_alpha}
 
-enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1 };
+enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2 };
 
 using GriT = MechT<MECH_GRI30_NSP, MECH_GRI30_NRXN, MECH_GRI30>;
 using H2T = MechT<MECH_H2O2_NSP, MECH_H2O2_NRXN, MECH_H2O2>;
+using NdT = MechT<MECH_NDODECANE_REITZ_NSP, MECH_NDODECANE_REITZ_NRXN, MECH_NDODECANE>;
 
 int mech_from_name(const char* name) {
     if (!name) return -1;
@@ -65,6 +67,7 @@ int mech_from_name(const char* name) {
     if (s.size() > 5 && s.substr(s.size() - 5) == ".yaml") s = s.substr(0, s.size() - 5);
     if (s == "gri30") return MECH_GRI30;
     if (s == "h2o2") return MECH_H2O2;
+    if (s == "nDodecane_Reitz") return MECH_NDODECANE;
     return -1;
 }
 
@@ -389,19 +392,19 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     return rc;
 }
 
-b200ode_status run(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
-    const bool fp64 = h->opt.precision == B200ODE_FP64;
-    if (h->mech == MECH_GRI30)
-        return fp64 ? launch_bdf<GriT, double>(h, p, st, launches) : launch_bdf<GriT, float>(h, p, st, launches);
-    return fp64 ? launch_bdf<H2T, double>(h, p, st, launches) : launch_bdf<H2T, float>(h, p, st, launches);
-}
-
 // Calls f(MT{}, LinT{}) with the handle's mechanism and Newton-matrix precision.
 template <class F>
 b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
     const bool fp64 = h->opt.precision == B200ODE_FP64;
     if (h->mech == MECH_GRI30) return fp64 ? f(GriT{}, double{}) : f(GriT{}, float{});
+    if (h->mech == MECH_NDODECANE) return fp64 ? f(NdT{}, double{}) : f(NdT{}, float{});
     return fp64 ? f(H2T{}, double{}) : f(H2T{}, float{});
+}
+
+b200ode_status run(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
+    return dispatch_mech(h, [&](auto mt, auto lt) {
+        return launch_bdf<decltype(mt), decltype(lt)>(h, p, st, launches);
+    });
 }
 
 // Launch shape of the persistent form: the same choice launch_bdf makes.
@@ -429,7 +432,7 @@ b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KP
 template <class MT, class LinT>
 b200ode_status launch_eval(b200ode_handle* h, KParams& p, double* d_dT, double* d_dY, double* d_jac,
                            cudaStream_t st) {
-    const int wpb = 4;
+    const int wpb = pick_wpb<MT, LinT>(h);   // shared memory per warp decides (4 for GRI, 1-2 for larger)
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
     const unsigned blocks = (unsigned)((p.ncells + wpb - 1) / wpb);
     if (d_jac) {
@@ -587,6 +590,7 @@ int32_t b200ode_mechanism_species(const char* mech_name) {
     switch (mech_from_name(mech_name)) {
         case MECH_GRI30: return MECH_GRI30_NSP;
         case MECH_H2O2: return MECH_H2O2_NSP;
+        case MECH_NDODECANE: return MECH_NDODECANE_REITZ_NSP;
         default: return -1;
     }
 }
@@ -598,7 +602,7 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     if (mech < 0)
         return fail(B200ODE_ERR_MECHANISM,
                     std::string("unknown mechanism '") + (mech_name ? mech_name : "(null)") +
-                        "' (available: gri30.yaml, h2o2.yaml)");
+                        "' (available: gri30.yaml, h2o2.yaml, nDodecane_Reitz.yaml)");
     b200ode_options o;
     b200ode_default_options(&o);
     if (opts) o = *opts;
@@ -617,7 +621,10 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     h->mech = mech;
     h->opt = o;
     std::string err;
-    h->hm = pack_mechanism(mech == MECH_GRI30 ? GEN_TABLES(gri30, MECH_GRI30) : GEN_TABLES(h2o2, MECH_H2O2), &err);
+    h->hm = pack_mechanism(mech == MECH_GRI30  ? GEN_TABLES(gri30, MECH_GRI30)
+                           : mech == MECH_H2O2 ? GEN_TABLES(h2o2, MECH_H2O2)
+                                               : GEN_TABLES(ndodecane_reitz, MECH_NDODECANE_REITZ),
+                           &err);
     if (h->hm.nsp == 0) {
         delete h;
         return fail(B200ODE_ERR_MECHANISM, "mechanism packing failed: " + err);
@@ -792,16 +799,12 @@ static b200ode_status eval_chem(b200ode_handle* h, int64_t n, const double* P, d
     double* d_out = nullptr;
     const size_t out_elems = jac ? (size_t)n * N * N : (size_t)n * (N - 1) + n;
     CUDA_TRY(cudaMallocAsync(&d_out, out_elems * sizeof(double), st));
-    const bool fp64 = h->opt.precision == B200ODE_FP64;
     double* d_dT = jac ? nullptr : d_out;
     double* d_dY = jac ? nullptr : d_out + n;
     double* d_jac = jac ? d_out : nullptr;
-    if (h->mech == MECH_GRI30)
-        rc = fp64 ? launch_eval<GriT, double>(h, p, d_dT, d_dY, d_jac, st)
-                  : launch_eval<GriT, float>(h, p, d_dT, d_dY, d_jac, st);
-    else
-        rc = fp64 ? launch_eval<H2T, double>(h, p, d_dT, d_dY, d_jac, st)
-                  : launch_eval<H2T, float>(h, p, d_dT, d_dY, d_jac, st);
+    rc = dispatch_mech(h, [&](auto mt, auto lt) {
+        return launch_eval<decltype(mt), decltype(lt)>(h, p, d_dT, d_dY, d_jac, st);
+    });
     if (rc == B200ODE_OK) {
         if (jac) {
             CUDA_TRY(cudaMemcpyAsync(jac, d_out, out_elems * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1051,13 +1054,9 @@ extern "C" b200ode_status b200ode_integrate_device_noalloc(b200ode_handle* h, in
     fill_params(h, p, n, dP, Ps, dT, dY, dstat, dcnt, t0, t1);
     int launches = 0;
     CUDA_TRY(cudaEventRecord(h->ev[1], st));
-    const bool fp64 = h->opt.precision == B200ODE_FP64;
-    if (h->mech == MECH_GRI30)
-        rc = fp64 ? launch_bdf_noalloc<GriT, double>(h, p, scratch, st, &launches)
-                  : launch_bdf_noalloc<GriT, float>(h, p, scratch, st, &launches);
-    else
-        rc = fp64 ? launch_bdf_noalloc<H2T, double>(h, p, scratch, st, &launches)
-                  : launch_bdf_noalloc<H2T, float>(h, p, scratch, st, &launches);
+    rc = dispatch_mech(h, [&](auto mt, auto lt) {
+        return launch_bdf_noalloc<decltype(mt), decltype(lt)>(h, p, scratch, st, &launches);
+    });
     if (rc != B200ODE_OK) return rc;
     CUDA_TRY(cudaEventRecord(h->ev[2], st));
     if (stats) {

@@ -363,7 +363,7 @@ __device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], con
             double acc = 0.0;
 #pragma unroll 1
             for (int j = 0; j < N; ++j) {
-                const double xj = __shfl_sync(kFull, (NS == 1 || j < 32) ? x.v[0] : x.v[NS - 1], j & 31);
+                const double xj = __shfl_sync(kFull, pick<NS>(x.v, j >> 5), j & 31);
                 if (i < N) acc += (double)wg->savedJ[i * N + j] * xj;
             }
             if (i < N) r.v[s] += S.gammap * acc;

@@ -44,7 +44,7 @@ struct MechT {
 };
 
 // Mechanism descriptors (one per compiled mechanism), set once per device.
-__constant__ DevMech c_mech[2];
+__constant__ DevMech c_mech[3];
 
 template <class MT>
 __device__ __forceinline__ const DevMech& mech() { return c_mech[MT::ID]; }
@@ -56,6 +56,21 @@ template <int NS>
 struct Vec {
     double v[NS];
 };
+
+// Element s of a lane's register slice (s not known at compile time): a select
+// chain over the NS registers instead of a local-memory index.
+template <int NS, class T>
+__device__ __forceinline__ T pick(const T (&x)[NS], int s) {
+    T r = x[0];
+#pragma unroll
+    for (int q = 1; q < NS; ++q) r = (s == q) ? x[q] : r;
+    return r;
+}
+template <int NS, class T>
+__device__ __forceinline__ void place(T (&x)[NS], int s, T v) {
+#pragma unroll
+    for (int q = 0; q < NS; ++q) if (s == q) x[q] = v;
+}
 
 // The kernels' dynamic shared memory.  Out-of-line phases receive byte offsets
 // into it (not pointers) and rebuild typed pointers here, so every access

@@ -33,9 +33,11 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
     LinT* A = smem_at<LinT>(A_off);
     int* perm = smem_at<int>(perm_off);
     LinT* dinv = smem_at<LinT>(dinv_off);
+    constexpr int NS = MT::NS;
     int sing = 0;
-    int pv = lane;   // lane i tracks perm[i] for i = lane, lane + 32
-    int pv2 = lane + 32;
+    int pv[NS];   // lane tracks perm[i] for i = lane + 32 s
+#pragma unroll
+    for (int s = 0; s < NS; ++s) pv[s] = lane + 32 * s;
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
         // pivot: first index of the max |a_ik|, i >= k
@@ -60,10 +62,10 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
                 A[bi * LDA + j] = t;
             }
             // compose the permutation: swap entries k and bi
-            const int ok = __shfl_sync(kFull, (k < 32) ? pv : pv2, k & 31);
-            const int ob = __shfl_sync(kFull, (bi < 32) ? pv : pv2, bi & 31);
-            if (lane == (k & 31)) { if (k < 32) pv = ob; else pv2 = ob; }
-            if (lane == (bi & 31)) { if (bi < 32) pv = ok; else pv2 = ok; }
+            const int ok = __shfl_sync(kFull, pick<NS>(pv, k >> 5), k & 31);
+            const int ob = __shfl_sync(kFull, pick<NS>(pv, bi >> 5), bi & 31);
+            if (lane == (k & 31)) place<NS>(pv, k >> 5, ob);
+            if (lane == (bi & 31)) place<NS>(pv, bi >> 5, ok);
             __syncwarp();
         }
         const LinT inv = LinT(1) / A[k * LDA + k];
@@ -80,8 +82,9 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
         }
         __syncwarp();
     }
-    if (lane < N) perm[lane] = pv;
-    if (lane + 32 < N) perm[lane + 32] = pv2;
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        if (lane + 32 * s < N) perm[lane + 32 * s] = pv[s];
     __syncwarp();
     return sing;
 }
@@ -115,8 +118,7 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
     // stay small in the instruction cache)
 #pragma unroll 1
     for (int k = 0; k < N - 1; ++k) {
-        const LinT src = (NS == 1 || k < 32) ? x[0] : x[NS - 1];
-        const LinT xk = __shfl_sync(kFull, src, k & 31);
+        const LinT xk = __shfl_sync(kFull, pick<NS>(x, k >> 5), k & 31);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + 32 * s;
@@ -126,12 +128,8 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
     // backward: upper
 #pragma unroll 1
     for (int k = N - 1; k >= 0; --k) {
-        const LinT src = (NS == 1 || k < 32) ? x[0] : x[NS - 1];
-        const LinT xk = __shfl_sync(kFull, src, k & 31) * dinv[k];
-        if (lane == (k & 31)) {
-            if (NS == 1 || k < 32) x[0] = xk;
-            else x[NS - 1] = xk;
-        }
+        const LinT xk = __shfl_sync(kFull, pick<NS>(x, k >> 5), k & 31) * dinv[k];
+        if (lane == (k & 31)) place<NS>(x, k >> 5, xk);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + 32 * s;

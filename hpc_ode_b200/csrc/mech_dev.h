@@ -212,7 +212,9 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
             int sp = g.prod_sp[r * P + i];
             if (sp < 0) break;
             for (int q = 0; q < g.prod_nu[r * P + i]; ++q) {
-                if (npf >= 3) { *err = "more than 3 product molecules"; return HostMech(); }
+                // product factors only enter the reverse rate
+                if (!g.rev[r]) continue;
+                if (npf >= 3) { *err = "more than 3 product molecules in a reversible reaction"; return HostMech(); }
                 pf[npf * ns + s] = sp; ++npf;
             }
             d += g.prod_nu[r * P + i];

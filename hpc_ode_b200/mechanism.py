@@ -411,7 +411,7 @@ MECH_DIR_ENV = "HPC_ODE_MECH_DIR"
 
 
 def load(name: str, mech_dir: Optional[str] = None) -> Mechanism:
-    """Parse ``<mech_dir>/<name>.yaml`` (``gri30``, ``h2o2``)."""
+    """Parse ``<mech_dir>/<name>.yaml`` (``gri30``, ``h2o2``, ``nDodecane_Reitz``)."""
     base = name[:-5] if name.endswith(".yaml") else name
     mech_dir = mech_dir or os.environ.get(MECH_DIR_ENV)
     if not mech_dir:
@@ -422,7 +422,7 @@ def load(name: str, mech_dir: Optional[str] = None) -> Mechanism:
 def generate_all(mech_dir: Optional[str] = None, out_dir: Optional[str] = None) -> List[str]:
     out_dir = out_dir or os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "mech")
     paths = []
-    for nm in ("gri30", "h2o2"):
+    for nm in ("gri30", "h2o2", "nDodecane_Reitz"):
         m = load(nm, mech_dir)
         p = os.path.join(out_dir, f"{nm}_mech.h")
         m.emit_header(p)

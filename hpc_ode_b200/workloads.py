@@ -13,6 +13,8 @@ Workloads (all rtol 1e-6, atol 1e-10):
   gri_bimodal  gri30, 262,144 cells, P = 101325 Pa, T0 70% U[300,900] / 30% U[1100,2200] K,
                phi log-uniform [0.3,3.0], dt 1e-4 s
   gri_1m       gri30, 1,048,576 cells, P ~ U[1,40] atm, T0 ~ U[900,2400] K, phi ~ U[0.4,2.5], dt 1e-4 s
+  nc12_8k      nDodecane_Reitz (100 species, 553 reactions), 8,192 cells, P ~ U[10,60] atm,
+               T0 ~ U[800,1600] K, n-dodecane/air phi ~ U[0.5,2.0], dt 1e-4 s
 """
 from __future__ import annotations
 
@@ -65,7 +67,7 @@ def premixed_Y(mech: str, fuel: str, phi: np.ndarray) -> np.ndarray:
     info = mech_info(mech)
     names = info["species"]
     mw = np.asarray(info["mw"])
-    idx = {s: i for i, s in enumerate(names)}
+    idx = {s.upper(): i for i, s in enumerate(names)}
     n = phi.size
     X = np.zeros((len(names), n))
     if fuel == "H2":
@@ -76,6 +78,11 @@ def premixed_Y(mech: str, fuel: str, phi: np.ndarray) -> np.ndarray:
         X[idx["CH4"]] = phi
         X[idx["O2"]] = 2.0
         X[idx["N2"]] = 7.52
+    elif fuel == "C12H26":
+        # C12H26 + 18.5 (O2 + 3.76 N2)
+        X[idx["C12H26"]] = phi
+        X[idx["O2"]] = 18.5
+        X[idx["N2"]] = 18.5 * 3.76
     else:
         raise ValueError(fuel)
     Ym = X * mw[:, None]
@@ -101,6 +108,12 @@ def make(name: str, ncells: Optional[int] = None, seed: Optional[int] = None) ->
         P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
         Y = premixed_Y("gri30", "CH4", phi)
         mech = "gri30"
+    elif kind == "ndodecane":
+        T = rng.uniform(cfg["T"][0], cfg["T"][1], n)
+        phi = rng.uniform(cfg["phi"][0], cfg["phi"][1], n)
+        P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
+        Y = premixed_Y("nDodecane_Reitz", "C12H26", phi)
+        mech = "nDodecane_Reitz"
     elif kind == "gri_bimodal":
         cold = rng.uniform(0.0, 1.0, n) < 0.7
         T = np.where(cold, rng.uniform(300.0, 900.0, n), rng.uniform(1100.0, 2200.0, n))
@@ -120,6 +133,9 @@ WORKLOADS = {
     "gri_bimodal": dict(kind="gri_bimodal", ncells=262144, dt=1e-4, seed=3),
     "gri_1m": dict(kind="gri", ncells=1048576, dt=1e-4, seed=5, T=(900.0, 2400.0),
                    phi=(0.4, 2.5), P_atm=(1.0, 40.0)),
+    # larger mechanism (100 species, 553 reactions): diesel-like n-dodecane/air
+    "nc12_8k": dict(kind="ndodecane", ncells=8192, dt=1e-4, seed=6, T=(800.0, 1600.0),
+                    phi=(0.5, 2.0), P_atm=(10.0, 60.0)),
 }
 RTOL, ATOL = 1e-6, 1e-10
 

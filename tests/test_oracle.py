@@ -55,7 +55,7 @@ def test_jacobian_TT_is_derivative_of_reference_rhs(oracle, golden_chem):
         assert abs(J[0, 0] - fd) <= 1e-5 * max(abs(fd), 1.0), (i, J[0, 0], fd)
 
 
-@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k")])
+@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k"), ("nDodecane_Reitz", "nc12_8k")])
 def test_jacobian_finite_difference(oracle, mech, wl):
     b = W.make(wl, 4, seed=7)
     ys = b.state_rows()

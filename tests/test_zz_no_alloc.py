@@ -71,3 +71,26 @@ def test_noalloc_rejects_bad_arguments():
             s.integrate_device_noalloc(-1, 0, 101325.0, 0, 0, 1e-4)
     finally:
         s.close()
+
+
+def test_noalloc_refuses_a_launch_larger_than_its_scratch():
+    """n-dodecane in FP64 keeps about 89 KB of scratch per resident warp; its
+    default launch (2 resident warps on each SM) needs more than the 24 MiB
+    array, so the call is refused with a message that gives the numbers, and the
+    allocating entry point still integrates the same cells."""
+    import torch
+    b = W.make("nc12_8k", 600, seed=3)
+    s = native.Solver("nDodecane_Reitz", precision=native.B200ODE_FP64)
+    try:
+        T = torch.from_numpy(b.T.copy()).cuda()
+        Y = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
+        P = torch.from_numpy(np.ascontiguousarray(b.P)).cuda()
+        with pytest.raises(native.B200Error) as e:
+            s.integrate_device_noalloc(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+        assert e.value.code == 1 and "static scratch holds" in str(e.value)
+        torch.cuda.synchronize()
+        assert torch.equal(T, torch.from_numpy(b.T).cuda())     # nothing ran
+        stats = s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+        assert stats["n_failed"] == 0
+    finally:
+        s.close()
