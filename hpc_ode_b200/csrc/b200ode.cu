@@ -26,6 +26,7 @@
 #include "mech/gri30_mech.h"
 #include "mech/h2o2_mech.h"
 #include "mech/nDodecane_Reitz_mech.h"
+#include "mech/h2_li_2004_mech.h"
 
 using namespace b200;
 
@@ -55,19 +56,22 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
               tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp,  \
               tag##_tb_alpha}
 
-enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2 };
+enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3 };
 
 using GriT = MechT<MECH_GRI30_NSP, MECH_GRI30_NRXN, MECH_GRI30>;
 using H2T = MechT<MECH_H2O2_NSP, MECH_H2O2_NRXN, MECH_H2O2>;
 using NdT = MechT<MECH_NDODECANE_REITZ_NSP, MECH_NDODECANE_REITZ_NRXN, MECH_NDODECANE>;
+using H2LiT = MechT<MECH_H2_LI_2004_NSP, MECH_H2_LI_2004_NRXN, MECH_H2LI>;
 
 int mech_from_name(const char* name) {
     if (!name) return -1;
     std::string s(name);
     if (s.size() > 5 && s.substr(s.size() - 5) == ".yaml") s = s.substr(0, s.size() - 5);
+    if (s.size() > 4 && s.substr(s.size() - 4) == ".xml") s = s.substr(0, s.size() - 4);
     if (s == "gri30") return MECH_GRI30;
     if (s == "h2o2") return MECH_H2O2;
     if (s == "nDodecane_Reitz") return MECH_NDODECANE;
+    if (s == "h2_li_2004") return MECH_H2LI;
     return -1;
 }
 
@@ -398,6 +402,7 @@ b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
     const bool fp64 = h->opt.precision == B200ODE_FP64;
     if (h->mech == MECH_GRI30) return fp64 ? f(GriT{}, double{}) : f(GriT{}, float{});
     if (h->mech == MECH_NDODECANE) return fp64 ? f(NdT{}, double{}) : f(NdT{}, float{});
+    if (h->mech == MECH_H2LI) return fp64 ? f(H2LiT{}, double{}) : f(H2LiT{}, float{});
     return fp64 ? f(H2T{}, double{}) : f(H2T{}, float{});
 }
 
@@ -591,6 +596,7 @@ int32_t b200ode_mechanism_species(const char* mech_name) {
         case MECH_GRI30: return MECH_GRI30_NSP;
         case MECH_H2O2: return MECH_H2O2_NSP;
         case MECH_NDODECANE: return MECH_NDODECANE_REITZ_NSP;
+        case MECH_H2LI: return MECH_H2_LI_2004_NSP;
         default: return -1;
     }
 }
@@ -602,7 +608,7 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     if (mech < 0)
         return fail(B200ODE_ERR_MECHANISM,
                     std::string("unknown mechanism '") + (mech_name ? mech_name : "(null)") +
-                        "' (available: gri30.yaml, h2o2.yaml, nDodecane_Reitz.yaml)");
+                        "' (available: gri30.yaml, h2o2.yaml, nDodecane_Reitz.yaml, h2_li_2004.xml)");
     b200ode_options o;
     b200ode_default_options(&o);
     if (opts) o = *opts;
@@ -623,6 +629,7 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     std::string err;
     h->hm = pack_mechanism(mech == MECH_GRI30  ? GEN_TABLES(gri30, MECH_GRI30)
                            : mech == MECH_H2O2 ? GEN_TABLES(h2o2, MECH_H2O2)
+                           : mech == MECH_H2LI ? GEN_TABLES(h2_li_2004, MECH_H2_LI_2004)
                                                : GEN_TABLES(ndodecane_reitz, MECH_NDODECANE_REITZ),
                            &err);
     if (h->hm.nsp == 0) {

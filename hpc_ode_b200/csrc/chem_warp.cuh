@@ -44,7 +44,7 @@ struct MechT {
 };
 
 // Mechanism descriptors (one per compiled mechanism), set once per device.
-__constant__ DevMech c_mech[3];
+__constant__ DevMech c_mech[4];
 
 template <class MT>
 __device__ __forceinline__ const DevMech& mech() { return c_mech[MT::ID]; }

@@ -220,76 +220,176 @@ class Mechanism:
             R = [(n, nu) for n, nu in R if n != "M"]
             if r.get("orders") or r.get("negative-A"):
                 raise NotImplementedError(f"reaction {i}: non-standard orders / negative A")
-            order = sum(nu for _, nu in L)
-            rx = Reaction(index=i, equation=eq, rtype=T_ELEMENTARY, reversible=rev,
-                          reac=[], prod=[])
-            effs = r.get("efficiencies", {})
-            default_eff = float(r.get("default-efficiency", 1.0))
-            if rtype_s in ("elementary",) and not has_M and falloff_m is None:
-                rc = r["rate-constant"]
-                rx.A = conv_A(float(rc["A"]), order)
-                rx.b = float(rc["b"])
-                rx.EaR = conv_Ea(float(rc["Ea"]))
-                # pyJac: in a termolecular step (three molecules on either
-                # side) a species found on both sides becomes the sole third
-                # body; bimolecular steps such as H + CH3O <=> H + CH2OH stay
-                # elementary (rxn_rates.c:764-766 vs rxn_rates_pres_mod.c:38).
-                lnames = {n for n, _ in L}
-                common = [n for n, _ in R if n in lnames]
-                termolecular = max(sum(nu for _, nu in L), sum(nu for _, nu in R)) >= 3
-                if common and termolecular:
-                    if len(common) != 1:
-                        raise NotImplementedError(f"reaction {i}: several catalysts")
-                    c = common[0]
-                    nl = dict(L)[c]
-                    nr = dict(R)[c]
-                    k = min(nl, nr)
-                    L = [(n, nu - (k if n == c else 0)) for n, nu in L]
-                    R = [(n, nu - (k if n == c else 0)) for n, nu in R]
-                    L = [(n, nu) for n, nu in L if nu > 0]
-                    R = [(n, nu) for n, nu in R if nu > 0]
-                    if k != 1:
-                        raise NotImplementedError(f"reaction {i}: catalyst count {k}")
-                    rx.rtype = T_THIRD_BODY
-                    rx.catalyst = idx[c]
-                    ci = idx[c]
-                    rx.tb = [(j, -1.0) for j in range(len(species)) if j != ci]
-            elif rtype_s == "three-body" or (has_M and rtype_s == "elementary"):
-                rc = r["rate-constant"]
-                rx.A = conv_A(float(rc["A"]), order + 1)
-                rx.b = float(rc["b"])
-                rx.EaR = conv_Ea(float(rc["Ea"]))
-                rx.rtype = T_THIRD_BODY
-                rx.tb = cls._tb_list(effs, default_eff, idx, len(species))
-            elif rtype_s == "falloff":
-                if falloff_m not in (None, "M"):
-                    raise NotImplementedError(f"reaction {i}: falloff with (+{falloff_m})")
-                lo_rc = r["low-P-rate-constant"]
-                hi_rc = r["high-P-rate-constant"]
-                rx.A = conv_A(float(hi_rc["A"]), order)
-                rx.b = float(hi_rc["b"])
-                rx.EaR = conv_Ea(float(hi_rc["Ea"]))
-                rx.A0 = conv_A(float(lo_rc["A"]), order + 1)
-                rx.b0 = float(lo_rc["b"])
-                rx.EaR0 = conv_Ea(float(lo_rc["Ea"]))
-                rx.tb = cls._tb_list(effs, default_eff, idx, len(species))
-                if "Troe" in r:
-                    t = r["Troe"]
-                    rx.rtype = T_TROE
-                    rx.troe = (float(t["A"]), float(t["T3"]), float(t["T1"]),
-                               float(t.get("T2", 0.0)))
-                    rx.troe_has_T2 = "T2" in t
-                elif "SRI" in r:
-                    raise NotImplementedError(f"reaction {i}: SRI falloff")
-                else:
-                    rx.rtype = T_LINDEMANN
+
+            def rate(which: str, order: int, r=r):
+                rc = r["rate-constant"] if which == "rate" else r[which]
+                return conv_A(float(rc["A"]), order), float(rc["b"]), conv_Ea(float(rc["Ea"]))
+
+            troe = None
+            if "Troe" in r:
+                t = r["Troe"]
+                troe = (float(t["A"]), float(t["T3"]), float(t["T1"]), float(t.get("T2", 0.0)), "T2" in t)
+            if "SRI" in r:
+                raise NotImplementedError(f"reaction {i}: SRI falloff")
+            if rtype_s == "three-body" or (has_M and rtype_s == "elementary"):
+                kind = "three-body"
+            elif rtype_s in ("elementary", "falloff"):
+                kind = rtype_s
             else:
                 raise NotImplementedError(f"reaction {i}: type {rtype_s}")
-            rx.reac = [(idx[n], nu) for n, nu in L]
-            rx.prod = [(idx[n], nu) for n, nu in R]
-            reactions.append(rx)
+            reactions.append(cls._make_reaction(
+                i, eq, rev, kind, L, R, falloff_m, rate, "rate", "high-P-rate-constant",
+                "low-P-rate-constant", troe, r.get("efficiencies", {}),
+                float(r.get("default-efficiency", 1.0)), idx, len(species)))
         nm = name or os.path.splitext(os.path.basename(path))[0]
         return cls(nm, species, reactions)
+
+    @classmethod
+    def from_ctml(cls, path: str, name: Optional[str] = None) -> "Mechanism":
+        """Parse a Cantera CTML (XML) mechanism: NASA-7 species, Arrhenius,
+        three-body and Lindemann/Troe falloff reactions.  CTML stores A in SI
+        kmol units and names E's unit on each element."""
+        import xml.etree.ElementTree as ET
+        root = ET.parse(path).getroot()
+        phase = root.find("phase")
+        sp_names = phase.find("speciesArray").text.split()
+        sp_el = {e.get("name"): e for e in root.iter("species")}
+        species: List[Species] = []
+        for nm in sp_names:
+            e = sp_el[nm]
+            comp = {}
+            for tok in (e.find("atomArray").text or "").split():
+                el, n = tok.split(":")
+                comp[el] = float(n)
+            mw = sum(ELEMENT_WEIGHTS[el] * n for el, n in comp.items())
+            polys = sorted(e.find("thermo").findall("NASA"), key=lambda x: float(x.get("Tmin")))
+            coeffs = [[float(v) for v in p.find("floatArray").text.replace(",", " ").split()] for p in polys]
+            if len(polys) == 1:
+                lo = hi = coeffs[0]
+                tmid = float(polys[0].get("Tmax"))
+            elif len(polys) == 2:
+                lo, hi = coeffs
+                tmid = float(polys[0].get("Tmax"))
+            else:
+                raise NotImplementedError(f"species {nm}: {len(polys)} NASA ranges")
+            species.append(Species(nm, mw, tmid, lo, hi))
+        idx = {s.name: i for i, s in enumerate(species)}
+        e_to_K = {"cal/mol": 4.184 / 8.3144621, "kcal/mol": 4184.0 / 8.3144621, "J/mol": 1.0 / 8.3144621,
+                  "kJ/mol": 1000.0 / 8.3144621, "J/kmol": 1.0 / 8314.4621, "K": 1.0}
+
+        def side(text: str) -> List[Tuple[str, int]]:
+            out = []
+            for tok in (text or "").split():
+                nm, nu = tok.rsplit(":", 1)
+                v = float(nu)
+                if v != int(v):
+                    raise NotImplementedError(f"non-integer stoichiometry: {tok}")
+                out.append((nm, int(v)))
+            return _merge(out)
+
+        reactions: List[Reaction] = []
+        for i, rxn in enumerate(root.iter("reaction")):
+            eq = rxn.find("equation").text
+            rev = rxn.get("reversible", "yes") == "yes"
+            t = rxn.get("type", "elementary")
+            rc = rxn.find("rateCoeff")
+            if rxn.find("order") is not None or rc.find("Arrhenius") is None or \
+                    rc.find("Arrhenius").get("type") == "stick":
+                raise NotImplementedError(f"reaction {i}: unsupported rate form")
+            arr = {a.get("name", "rate"): a for a in rc.findall("Arrhenius")}
+
+            def rate(which: str, order: int, arr=arr):
+                a = arr["k0" if which == "low" else "rate"]
+                A = float(a.find("A").text)
+                if A < 0:
+                    raise NotImplementedError("negative A")
+                Ee = a.find("E")
+                return A, float(a.find("b").text), float(Ee.text) * e_to_K[Ee.get("units", "cal/mol")]
+
+            troe = None
+            fo = rc.find("falloff")
+            if fo is not None:
+                if fo.get("type") == "Troe":
+                    v = [float(x) for x in fo.text.split()]
+                    troe = (v[0], v[1], v[2], v[3] if len(v) > 3 else 0.0, len(v) > 3)
+                elif fo.get("type") != "Lindemann":
+                    raise NotImplementedError(f"reaction {i}: falloff {fo.get('type')}")
+            effs, default_eff = {}, 1.0
+            ef = rc.find("efficiencies")
+            if ef is not None:
+                default_eff = float(ef.get("default", "1.0"))
+                for tok in (ef.text or "").split():
+                    nm, v = tok.rsplit(":", 1)
+                    effs[nm] = float(v)
+            if t == "threeBody":
+                kind = "three-body"
+            elif t == "falloff":
+                kind = "falloff"
+            elif t == "elementary":
+                kind = "elementary"
+            else:
+                raise NotImplementedError(f"reaction {i}: type {t}")
+            L, R = side(rxn.find("reactants").text), side(rxn.find("products").text)
+            reactions.append(cls._make_reaction(
+                i, eq, rev, kind, L, R, "M" if kind == "falloff" else None, rate, "rate", "rate", "low",
+                troe, effs, default_eff, idx, len(species)))
+        nm = name or os.path.splitext(os.path.basename(path))[0]
+        return cls(nm, species, reactions)
+
+    @classmethod
+    def _make_reaction(cls, i, eq, rev, kind, L, R, falloff_m, rate, k_elem, k_hi, k_lo, troe, effs,
+                       default_eff, idx, nsp) -> Reaction:
+        """One reaction with pyJac's conventions.  rate(key, order) gives
+        (A [SI kmol units], b, Ea/R [K]) for the rate expression named key."""
+        order = sum(nu for _, nu in L)
+        rx = Reaction(index=i, equation=eq, rtype=T_ELEMENTARY, reversible=rev, reac=[], prod=[])
+        if kind == "elementary":
+            rx.A, rx.b, rx.EaR = rate(k_elem, order)
+            # pyJac: in a termolecular step (three molecules on either
+            # side) a species found on both sides becomes the sole third
+            # body; bimolecular steps such as H + CH3O <=> H + CH2OH stay
+            # elementary (rxn_rates.c:764-766 vs rxn_rates_pres_mod.c:38).
+            lnames = {n for n, _ in L}
+            common = [n for n, _ in R if n in lnames]
+            termolecular = max(sum(nu for _, nu in L), sum(nu for _, nu in R)) >= 3
+            if common and termolecular:
+                if len(common) != 1:
+                    raise NotImplementedError(f"reaction {i}: several catalysts")
+                c = common[0]
+                nl = dict(L)[c]
+                nr = dict(R)[c]
+                k = min(nl, nr)
+                L = [(n, nu - (k if n == c else 0)) for n, nu in L]
+                R = [(n, nu - (k if n == c else 0)) for n, nu in R]
+                L = [(n, nu) for n, nu in L if nu > 0]
+                R = [(n, nu) for n, nu in R if nu > 0]
+                if k != 1:
+                    raise NotImplementedError(f"reaction {i}: catalyst count {k}")
+                rx.rtype = T_THIRD_BODY
+                rx.catalyst = idx[c]
+                ci = idx[c]
+                rx.tb = [(j, -1.0) for j in range(nsp) if j != ci]
+        elif kind == "three-body":
+            rx.A, rx.b, rx.EaR = rate(k_elem, order + 1)
+            rx.rtype = T_THIRD_BODY
+            rx.tb = cls._tb_list(effs, default_eff, idx, nsp)
+        elif kind == "falloff":
+            if falloff_m not in (None, "M"):
+                raise NotImplementedError(f"reaction {i}: falloff with (+{falloff_m})")
+            rx.A, rx.b, rx.EaR = rate(k_hi, order)
+            rx.A0, rx.b0, rx.EaR0 = rate(k_lo, order + 1)
+            rx.tb = cls._tb_list(effs, default_eff, idx, nsp)
+            if troe is not None:
+                rx.rtype = T_TROE
+                rx.troe = troe[:4]
+                rx.troe_has_T2 = troe[4]
+            else:
+                rx.rtype = T_LINDEMANN
+        else:
+            raise NotImplementedError(f"reaction {i}: type {kind}")
+        rx.reac = [(idx[n], nu) for n, nu in L]
+        rx.prod = [(idx[n], nu) for n, nu in R]
+        return rx
 
     @staticmethod
     def _tb_list(effs, default_eff, idx, nsp) -> List[Tuple[int, float]]:
@@ -411,18 +511,22 @@ MECH_DIR_ENV = "HPC_ODE_MECH_DIR"
 
 
 def load(name: str, mech_dir: Optional[str] = None) -> Mechanism:
-    """Parse ``<mech_dir>/<name>.yaml`` (``gri30``, ``h2o2``, ``nDodecane_Reitz``)."""
-    base = name[:-5] if name.endswith(".yaml") else name
+    """Parse ``<mech_dir>/<name>.yaml``, or ``<name>.xml`` (CTML) when there is
+    no YAML file (``gri30``, ``h2o2``, ``nDodecane_Reitz``, ``h2_li_2004``)."""
+    base = os.path.splitext(name)[0] if name.endswith((".yaml", ".xml")) else name
     mech_dir = mech_dir or os.environ.get(MECH_DIR_ENV)
     if not mech_dir:
         raise RuntimeError(f"set {MECH_DIR_ENV} to the directory holding {base}.yaml")
-    return Mechanism.from_yaml(os.path.join(mech_dir, base + ".yaml"), base)
+    yml = os.path.join(mech_dir, base + ".yaml")
+    if os.path.exists(yml):
+        return Mechanism.from_yaml(yml, base)
+    return Mechanism.from_ctml(os.path.join(mech_dir, base + ".xml"), base)
 
 
 def generate_all(mech_dir: Optional[str] = None, out_dir: Optional[str] = None) -> List[str]:
     out_dir = out_dir or os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "mech")
     paths = []
-    for nm in ("gri30", "h2o2", "nDodecane_Reitz"):
+    for nm in ("gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004"):
         m = load(nm, mech_dir)
         p = os.path.join(out_dir, f"{nm}_mech.h")
         m.emit_header(p)

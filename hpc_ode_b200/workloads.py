@@ -13,6 +13,8 @@ Workloads (all rtol 1e-6, atol 1e-10):
   gri_bimodal  gri30, 262,144 cells, P = 101325 Pa, T0 70% U[300,900] / 30% U[1100,2200] K,
                phi log-uniform [0.3,3.0], dt 1e-4 s
   gri_1m       gri30, 1,048,576 cells, P ~ U[1,40] atm, T0 ~ U[900,2400] K, phi ~ U[0.4,2.5], dt 1e-4 s
+  h2li_grid    h2_li_2004 (9 species, 21 reactions), 10,000 cells: the reference H2 dataset's grid,
+               T0 = linspace(1000,2100,100) x phi = linspace(0.5,3.5,100), P = 101325.15 Pa, dt 1e-3 s
   nc12_8k      nDodecane_Reitz (100 species, 553 reactions), 8,192 cells, P ~ U[10,60] atm,
                T0 ~ U[800,1600] K, n-dodecane/air phi ~ U[0.5,2.0], dt 1e-4 s
 """
@@ -108,6 +110,16 @@ def make(name: str, ncells: Optional[int] = None, seed: Optional[int] = None) ->
         P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
         Y = premixed_Y("gri30", "CH4", phi)
         mech = "gri30"
+    elif kind == "h2_grid":
+        # the reference's H2 dataset layout: a 100 x 100 grid of T (outer) and
+        # phi (inner) at 1 atm; n < 10,000 takes evenly spaced grid points
+        Tg, pg = np.meshgrid(np.linspace(1000.0, 2100.0, 100), np.linspace(0.5, 3.5, 100), indexing="ij")
+        pick = np.linspace(0, Tg.size - 1, n).round().astype(int) if n <= Tg.size else np.arange(n) % Tg.size
+        T = Tg.ravel()[pick].copy()
+        phi = pg.ravel()[pick].copy()
+        P = np.full(n, cfg["P"])
+        Y = premixed_Y("h2_li_2004", "H2", phi)
+        mech = "h2_li_2004"
     elif kind == "ndodecane":
         T = rng.uniform(cfg["T"][0], cfg["T"][1], n)
         phi = rng.uniform(cfg["phi"][0], cfg["phi"][1], n)
@@ -133,6 +145,8 @@ WORKLOADS = {
     "gri_bimodal": dict(kind="gri_bimodal", ncells=262144, dt=1e-4, seed=3),
     "gri_1m": dict(kind="gri", ncells=1048576, dt=1e-4, seed=5, T=(900.0, 2400.0),
                    phi=(0.4, 2.5), P_atm=(1.0, 40.0)),
+    # the reference's H2 dataset grid with its Li et al. (2004) mechanism (9 species, 21 reactions)
+    "h2li_grid": dict(kind="h2_grid", ncells=10000, dt=1e-3, seed=7, P=101325.15),
     # larger mechanism (100 species, 553 reactions): diesel-like n-dodecane/air
     "nc12_8k": dict(kind="ndodecane", ncells=8192, dt=1e-4, seed=6, T=(800.0, 1600.0),
                     phi=(0.5, 2.0), P_atm=(10.0, 60.0)),

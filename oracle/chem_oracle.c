@@ -22,6 +22,7 @@
 #include "../hpc_ode_b200/csrc/mech/gri30_mech.h"
 #include "../hpc_ode_b200/csrc/mech/h2o2_mech.h"
 #include "../hpc_ode_b200/csrc/mech/nDodecane_Reitz_mech.h"
+#include "../hpc_ode_b200/csrc/mech/h2_li_2004_mech.h"
 
 #define RU 8314.4621
 #define PATM 101325.0
@@ -43,19 +44,21 @@ typedef struct {
     tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp, \
     tag##_tb_alpha }
 
-static const mech_t MECHS[3] = { MECH_INIT(gri30, MECH_GRI30), MECH_INIT(h2o2, MECH_H2O2),
-                                 MECH_INIT(ndodecane_reitz, MECH_NDODECANE_REITZ) };
+static const mech_t MECHS[4] = { MECH_INIT(gri30, MECH_GRI30), MECH_INIT(h2o2, MECH_H2O2),
+                                 MECH_INIT(ndodecane_reitz, MECH_NDODECANE_REITZ),
+                                 MECH_INIT(h2_li_2004, MECH_H2_LI_2004) };
 
 int oracle_mech_id(const char* name) {
     if (!name) return -1;
     if (!strncmp(name, "gri30", 5)) return ORACLE_MECH_GRI30;
     if (!strncmp(name, "h2o2", 4)) return ORACLE_MECH_H2O2;
     if (!strncmp(name, "nDodecane_Reitz", 15)) return ORACLE_MECH_NDODECANE;
+    if (!strncmp(name, "h2_li_2004", 10)) return ORACLE_MECH_H2LI;
     return -1;
 }
 
 int oracle_mech_nsp(int mech) {
-    if (mech < 0 || mech > 2) return -1;
+    if (mech < 0 || mech > 3) return -1;
     return MECHS[mech].nsp;
 }
 
@@ -380,3 +383,5 @@ void oracle_h2o2_dydt(double t, double pres, const double* y, double* dy) { (voi
 void oracle_h2o2_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_H2O2, pres, y, jac); }
 void oracle_ndodecane_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_NDODECANE, pres, y, dy); }
 void oracle_ndodecane_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_NDODECANE, pres, y, jac); }
+void oracle_h2li_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_H2LI, pres, y, dy); }
+void oracle_h2li_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_H2LI, pres, y, jac); }

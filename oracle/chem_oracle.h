@@ -22,7 +22,7 @@ extern "C" {
 #endif
 
 /* Mechanism ids. */
-enum { ORACLE_MECH_GRI30 = 0, ORACLE_MECH_H2O2 = 1, ORACLE_MECH_NDODECANE = 2 };
+enum { ORACLE_MECH_GRI30 = 0, ORACLE_MECH_H2O2 = 1, ORACLE_MECH_NDODECANE = 2, ORACLE_MECH_H2LI = 3 };
 
 int oracle_mech_id(const char* name);      /* "gri30"/"gri30.yaml"/"h2o2"... ; -1 if unknown */
 int oracle_mech_nsp(int mech);             /* number of species == state length */
@@ -34,6 +34,8 @@ void oracle_h2o2_dydt(double t, double pres, const double* y, double* dy);
 void oracle_h2o2_jacob(double t, double pres, const double* y, double* jac);
 void oracle_ndodecane_dydt(double t, double pres, const double* y, double* dy);
 void oracle_ndodecane_jacob(double t, double pres, const double* y, double* jac);
+void oracle_h2li_dydt(double t, double pres, const double* y, double* dy);
+void oracle_h2li_jacob(double t, double pres, const double* y, double* jac);
 
 /* Generic forms. */
 void oracle_dydt(int mech, double pres, const double* y, double* dy);

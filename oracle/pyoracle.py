@@ -40,7 +40,7 @@ STATS_DTYPE = np.dtype([("status", "i4"), ("nst", "i4"), ("nfe", "i4"), ("nje", 
                         ("qlast", "i4"), ("pad", "i4"), ("hlast", "f8")])
 assert STATS_DTYPE.itemsize == C.sizeof(BdfStats)
 
-MECH_IDS = {"gri30": 0, "h2o2": 1, "nDodecane_Reitz": 2}
+MECH_IDS = {"gri30": 0, "h2o2": 1, "nDodecane_Reitz": 2, "h2_li_2004": 3}
 
 
 def build(force: bool = False) -> None:

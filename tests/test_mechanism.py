@@ -1,0 +1,68 @@
+"""Mechanism table generation (hpc_ode_b200/mechanism.py), on the CPU.
+
+Reads the reference's mechanism files where they lie (skipped when the
+reference checkout is absent): the committed tables must be what the generator
+produces, and the CTML (XML) reader must give the same mechanism as the YAML
+reader for the mechanisms the reference ships in both forms."""
+import os
+
+import numpy as np
+import pytest
+
+from hpc_ode_b200 import mechanism as M
+from hpc_ode_b200 import workloads as W
+
+REF_MECH = "/root/reference/resources/mechanisms"
+REF_DATA = "/root/reference/ref_data"
+needs_ref = pytest.mark.skipif(not os.path.isdir(REF_MECH), reason="reference mechanisms not present")
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004"])
+def test_committed_tables_are_generated(tmp_path, name):
+    m = M.load(name, REF_MECH)
+    out = tmp_path / f"{name}_mech.h"
+    m.emit_header(str(out))
+    committed = os.path.join(os.path.dirname(M.__file__), "csrc", "mech", f"{name}_mech.h")
+    assert open(out).read() == open(committed).read()
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["gri30", "nDodecane_Reitz"])
+def test_ctml_reader_matches_yaml_reader(name):
+    a = M.Mechanism.from_yaml(os.path.join(REF_MECH, name + ".yaml"), name)
+    b = M.Mechanism.from_ctml(os.path.join(REF_MECH, name + ".xml"), name)
+    assert a.counts() == b.counts()
+    assert [s.name for s in a.species] == [s.name for s in b.species]
+    for sa, sb in zip(a.species, b.species):
+        assert sa.tmid == sb.tmid and sa.lo == sb.lo and sa.hi == sb.hi
+        assert abs(sa.mw - sb.mw) <= 1e-12 * sa.mw
+    for ra, rb in zip(a.reactions, b.reactions):
+        assert (ra.reac, ra.prod, ra.rtype, ra.reversible, ra.tb, ra.troe_has_T2) == \
+               (rb.reac, rb.prod, rb.rtype, rb.reversible, rb.tb, rb.troe_has_T2), ra.equation
+        for f in ("A", "b", "EaR", "A0", "b0", "EaR0"):
+            x, y = getattr(ra, f), getattr(rb, f)
+            assert abs(x - y) <= 1e-15 * max(abs(x), abs(y)), (ra.equation, f, x, y)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_DATA, "res_h2.csv")), reason="reference data not present")
+def test_h2_grid_workload_reproduces_reference_dataset():
+    ref = np.genfromtxt(os.path.join(REF_DATA, "res_h2.csv"), delimiter=",", names=True)
+    b = W.make("h2li_grid")
+    assert b.ncells == ref.size == 10000
+    assert np.array_equal(b.T, ref["TEMPE"])
+    Y = np.stack([ref[f"CO{k}"] for k in range(9)])
+    assert np.abs(b.Y - Y).max() <= 1e-15
+
+
+def test_unsupported_forms_raise(tmp_path):
+    p = tmp_path / "bad.xml"
+    p.write_text("""<ctml><phase id="gas"><speciesArray>A</speciesArray></phase>
+<speciesData><species name="A"><atomArray>H:1</atomArray><thermo>
+<NASA Tmin="300" Tmax="1000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA>
+<NASA Tmin="1000" Tmax="5000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA></thermo></species></speciesData>
+<reactionData><reaction id="1" type="plog"><equation>A =] A</equation><rateCoeff><Arrhenius><A>1</A><b>0</b>
+<E units="K">0</E></Arrhenius></rateCoeff><reactants>A:1</reactants><products>A:1</products></reaction>
+</reactionData></ctml>""")
+    with pytest.raises(NotImplementedError):
+        M.Mechanism.from_ctml(str(p), "bad")
