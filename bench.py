@@ -39,7 +39,7 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per cell of one k_bdf launch, from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, 8,192-cell GRI capture, mixed precision): the traffic
 # is the compulsory T/P/Y in + T/Y/status out, so it scales with the cell count.
-NCU_DRAM_BYTES_PER_CELL = {"gri30": 861.0}
+NCU_DRAM_BYTES_PER_CELL = {"gri30": 856.0}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
