@@ -11,6 +11,7 @@
 //     launches (k_bdf with per-cell records);
 //   * state in HBM is structure-of-arrays with the cell index innermost.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -35,6 +36,13 @@ namespace {
 thread_local std::string g_last_error;
 std::mutex g_tables_mu;
 std::map<std::pair<int, int>, unsigned char*> g_tables;   // (device, mechanism) -> tables
+
+// Host-side NVTX range for profilers (Nsight Systems): one per entry point and
+// per phase it enqueues.  Header-only NVTX: no cost when no tool is attached.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
 
 b200ode_status fail(b200ode_status st, const std::string& msg) {
     g_last_error = msg;
@@ -692,6 +700,7 @@ void b200ode_destroy(b200ode_handle* h) {
 b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n, const double* dP, double Ps,
                                         double* dT, double* dY, double t0, double t1, int32_t* dstat,
                                         b200ode_stats* stats, void* stream) {
+    NvtxRange range("b200ode_integrate_device");
     b200ode_status rc = check_args(h, n, t0, t1);
     if (rc != B200ODE_OK) return rc;
     if (n == 0) {
@@ -727,6 +736,7 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n, const doub
 b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n, const double* P, double Ps, double* T,
                                  double* Y, double t0, double t1, int32_t* cell_status,
                                  b200ode_stats* stats) {
+    NvtxRange range("b200ode_integrate");
     b200ode_status rc = check_args(h, n, t0, t1);
     if (rc != B200ODE_OK) return rc;
     if (n == 0) {
@@ -746,11 +756,14 @@ b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n, const double* P, 
     const size_t nsp = h->hm.nsp;
     const bool want_cnt = stats && (stats->nst || stats->nfe || stats->nje || stats->nsetups ||
                                     stats->nni || stats->ncfn || stats->netf);
+    {
+    NvtxRange h2d_range("h2d");
     CUDA_TRY(cudaEventRecord(h->ev[0], st));
     CUDA_TRY(cudaMemcpyAsync(h->d_T, T, n * sizeof(double), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaMemcpyAsync(h->d_Y, Y, n * nsp * sizeof(double), cudaMemcpyHostToDevice, st));
     if (P) CUDA_TRY(cudaMemcpyAsync(h->d_P, P, n * sizeof(double), cudaMemcpyHostToDevice, st));
     CUDA_TRY(cudaEventRecord(h->ev[1], st));
+    }
     int32_t* dcnt[7];
     for (int i = 0; i < 7; ++i) dcnt[i] = want_cnt ? h->d_cnt + (size_t)i * n : nullptr;
     KParams p;
@@ -771,7 +784,10 @@ b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n, const double* P, 
                                          cudaMemcpyDeviceToHost, st));
     }
     CUDA_TRY(cudaEventRecord(h->ev[3], st));
-    CUDA_TRY(cudaStreamSynchronize(st));
+    {
+        NvtxRange wait("device (copies + BDF kernel)");
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
     if (stats) {
         rc = read_totals(h, stats, st);
         if (rc != B200ODE_OK) return rc;

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <sstream>
 #include <stdexcept>
+#include <string>
 
 #include "b200ode_integrator.hpp"
 
@@ -22,6 +23,62 @@ B200BDFIntegrator::~B200BDFIntegrator() {
 
 void B200BDFIntegrator::setOptions(const b200ode_options& opts) { opts_ = opts; }
 
+namespace {
+
+// One solver option from the integrator config.  With the reference's headers
+// the app passes config["integrator"]["omp"] as ompConfig, so the options sit
+// under integrator.omp.b200.<key> in its YAML; the restated interface keeps
+// them as "b200.<key>" entries of the ompConfig map.
+bool cfg_get(const IntegratorConfig& c, const char* key, std::string* out) {
+#ifdef B200ODE_WITH_REFERENCE_HEADERS
+    const YAML::Node n = c.ompConfig["b200"];
+    if (!n || !n[key]) return false;
+    *out = n[key].as<std::string>();
+    return true;
+#else
+    auto it = c.ompConfig.find(std::string("b200.") + key);
+    if (it == c.ompConfig.end()) return false;
+    *out = it->second;
+    return true;
+#endif
+}
+
+int cfg_int(const std::string& key, const std::string& v) {
+    try {
+        size_t pos = 0;
+        const int x = std::stoi(v, &pos);
+        if (pos == v.size()) return x;
+    } catch (...) {
+    }
+    throw std::runtime_error("b200." + key + ": not an integer: '" + v + "'");
+}
+
+// Applies the b200 options of the config: precision (fp64 | mixed), refine (0 | 1),
+// max_steps, max_order, form (persistent | step), graph (0 | 1), warps_per_block,
+// blocks_per_sm, device.  Unknown values throw std::runtime_error.
+void apply_config(const IntegratorConfig& c, b200ode_options* o) {
+    std::string v;
+    if (cfg_get(c, "precision", &v)) {
+        if (v == "fp64") o->precision = B200ODE_FP64;
+        else if (v == "mixed") o->precision = B200ODE_MIXED;
+        else throw std::runtime_error("b200.precision must be fp64 or mixed, not '" + v + "'");
+    }
+    if (cfg_get(c, "form", &v)) {
+        if (v == "persistent") o->persistent = 1;
+        else if (v == "step") o->persistent = 0;
+        else throw std::runtime_error("b200.form must be persistent or step, not '" + v + "'");
+    }
+    if (cfg_get(c, "refine", &v)) o->refine = cfg_int("refine", v);
+    if (cfg_get(c, "max_steps", &v)) o->max_steps = cfg_int("max_steps", v);
+    if (cfg_get(c, "max_order", &v)) o->max_order = cfg_int("max_order", v);
+    if (cfg_get(c, "graph", &v)) o->use_graph = cfg_int("graph", v);
+    if (cfg_get(c, "warps_per_block", &v)) o->warps_per_block = cfg_int("warps_per_block", v);
+    if (cfg_get(c, "blocks_per_sm", &v)) o->blocks_per_sm = cfg_int("blocks_per_sm", v);
+    if (cfg_get(c, "device", &v)) o->device = cfg_int("device", v);
+}
+
+}  // namespace
+
 void B200BDFIntegrator::init(std::shared_ptr<Context> c, IntegratorConfig config) {
     Integrator::init(std::move(c), config);
     // mechanism check before any device work (CVodeIntegrator.cpp:41-48)
@@ -35,6 +92,12 @@ void B200BDFIntegrator::init(std::shared_ptr<Context> c, IntegratorConfig config
     if (handle_) b200ode_destroy(handle_);
     handle_ = nullptr;
     b200ode_options o = opts_;
+    try {
+        apply_config(config, &o);
+    } catch (const std::exception& e) {
+        logger->error(e.what());
+        throw;
+    }
     o.reltol = reltol;
     o.abstol = abstol;
     const b200ode_status rc = b200ode_create(mechanism.c_str(), &o, &handle_);

@@ -3,7 +3,7 @@
 // string, runs init / integrate(0, dt) / clean as the reference's application
 // does (app/main.cpp), and writes the mesh back.
 //
-//   integrator_driver <type> <mechanism> <in.bin> <out.bin>
+//   integrator_driver <type> <mechanism> <in.bin> <out.bin> [b200.key=value ...]
 // in.bin:  int32 n, int32 nsp, double dt, double pressure, double T[n], double Y[n][nsp]
 // out.bin: the same layout after integration, then int32 status[n]
 // Exit 0 on success; on an exception prints "EXCEPTION: <what>" and exits 3.
@@ -13,13 +13,14 @@
 #include <fstream>
 #include <iostream>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "b200ode_integrator.hpp"
 
 int main(int argc, char** argv) {
-    if (argc != 5) {
-        std::fprintf(stderr, "usage: %s <type> <mechanism> <in.bin> <out.bin>\n", argv[0]);
+    if (argc < 5) {
+        std::fprintf(stderr, "usage: %s <type> <mechanism> <in.bin> <out.bin> [b200.key=value ...]\n", argv[0]);
         return 2;
     }
     try {
@@ -41,6 +42,12 @@ int main(int argc, char** argv) {
         auto ctx = std::make_shared<Context>(logger, mesh);
         std::unique_ptr<Integrator> integrator = createIntegrator(argv[1]);
         IntegratorConfig config{argv[2], 1.0e-6, 1.0e-10, P, {}};
+        for (int a = 5; a < argc; ++a) {   // config options, as the app's YAML would give them
+            const std::string kv = argv[a];
+            const size_t eq = kv.find('=');
+            if (eq == std::string::npos) throw std::runtime_error("option without '=': " + kv);
+            config.ompConfig[kv.substr(0, eq)] = kv.substr(eq + 1);
+        }
         integrator->init(ctx, config);
         integrator->integrate(0.0, dt);
         auto* b200 = dynamic_cast<B200BDFIntegrator*>(integrator.get());

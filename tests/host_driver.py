@@ -20,7 +20,7 @@ def build(tmpdir) -> str:
     return exe
 
 
-def run(exe, tmpdir, itype, mech, T, Y_rows, dt, P):
+def run(exe, tmpdir, itype, mech, T, Y_rows, dt, P, options=()):
     """T[n], Y_rows[n, nsp] (cell-major, as the reference's Mesh). Returns
     (returncode, stdout, T_out, Y_out, status) with outputs None on failure."""
     n, nsp = Y_rows.shape
@@ -31,7 +31,7 @@ def run(exe, tmpdir, itype, mech, T, Y_rows, dt, P):
         f.write(np.array([dt, P], dtype=np.float64).tobytes())
         f.write(np.ascontiguousarray(T, dtype=np.float64).tobytes())
         f.write(np.ascontiguousarray(Y_rows, dtype=np.float64).tobytes())
-    r = subprocess.run([exe, itype, mech, fin, fout], capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe, itype, mech, fin, fout, *options], capture_output=True, text=True, timeout=600)
     if r.returncode != 0:
         return r.returncode, r.stdout, None, None, None
     raw = open(fout, "rb").read()

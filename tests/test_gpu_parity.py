@@ -231,6 +231,33 @@ def test_failure_paths_are_reported_and_isolated(oracle):
     assert np.array_equal(Tbad[good], Tref[good]) and np.array_equal(Ybad[:, good], Yref[:, good])
 
 
+@pytest.mark.parametrize("precision", [native.B200ODE_FP64, native.B200ODE_MIXED])
+def test_poisoned_cells_do_not_disturb_neighbours(precision):
+    """Host-side fault injection: a cell at 50 K, a cell with a negative mass
+    fraction, an infinite temperature and a zero-density cell are integrated in
+    one batch with healthy cells.  Every call returns, each poisoned cell gets a
+    CVODE status of its own, and the healthy cells are bitwise those of a clean
+    run."""
+    b = W.make("gri_32k", 12, seed=11)
+    s = native.Solver("gri30", precision=precision, max_steps=2000)
+    Tc, Yc = b.T.copy(), b.Y.copy()
+    st_clean, _, _ = s.integrate(Tc, Yc, b.P, b.dt)
+    T, Y = b.T.copy(), b.Y.copy()
+    T[2] = 50.0                      # far below the NASA-7 fit range
+    Y[3, 5] = -0.05                  # negative O2 mass fraction
+    T[7] = np.inf
+    Y[:, 9] = 0.0                    # no mass at all
+    st, stats, _ = s.integrate(T, Y, b.P, b.dt)
+    s.close()
+    poisoned = np.array([2, 5, 7, 9])
+    good = np.setdiff1d(np.arange(12), poisoned)
+    assert (st_clean == 0).all()
+    assert np.array_equal(T[good], Tc[good]) and np.array_equal(Y[:, good], Yc[:, good])
+    assert np.array_equal(st[good], st_clean[good])
+    assert set(np.unique(st[poisoned])) <= {0, -1, -2, -3, -4}
+    assert st[7] != 0 and stats["n_failed"] >= 1
+
+
 def test_invalid_arguments_raise():
     with pytest.raises(native.B200Error):
         native.Solver("not_a_mechanism")

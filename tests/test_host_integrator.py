@@ -39,6 +39,17 @@ def test_mechanism_size_mismatch_throws_before_device_work(driver):
     assert rc == 3 and "(-1) differs" in out
 
 
+def test_bad_b200_options_throw_before_device_work(driver):
+    exe, d = driver
+    T, Y = _cells()
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0,
+                                  ["b200.precision=fp16"])
+    assert rc == 3 and "b200.precision must be fp64 or mixed" in out
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0,
+                                  ["b200.max_steps=lots"])
+    assert rc == 3 and "b200.max_steps: not an integer" in out
+
+
 def test_no_device_is_a_runtime_error(driver):
     import torch
     if torch.cuda.is_available():
@@ -64,14 +75,18 @@ def test_quiescent_reference_case_through_cpp(driver, golden_e2e):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("wl,mech", [("gri_32k", "gri30.yaml"), ("h2_1024", "h2o2.yaml")])
-def test_reacting_cells_match_c_abi(driver, wl, mech):
+@pytest.mark.parametrize("wl,mech,opts,precision", [
+    ("gri_32k", "gri30.yaml", [], native.B200ODE_MIXED),
+    ("h2_1024", "h2o2.yaml", [], native.B200ODE_MIXED),
+    ("gri_32k", "gri30.yaml", ["b200.precision=fp64", "b200.form=step"], native.B200ODE_FP64),
+    ("h2li_grid", "h2_li_2004.xml", [], native.B200ODE_MIXED)])
+def test_reacting_cells_match_c_abi(driver, wl, mech, opts, precision):
     exe, d = driver
     b = W.make(wl, 48, seed=77)
     P = float(b.P[0])
-    rc, out, To, Yo, st = host_driver.run(exe, d, "BDFIntegratorB200", mech, b.T, b.Y.T, b.dt, P)
+    rc, out, To, Yo, st = host_driver.run(exe, d, "BDFIntegratorB200", mech, b.T, b.Y.T, b.dt, P, opts)
     assert rc == 0, out
-    s = native.Solver(b.mech)
+    s = native.Solver(b.mech, precision=precision)
     T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
     st2, _, _ = s.integrate(T, Y, P, b.dt)
     s.close()
