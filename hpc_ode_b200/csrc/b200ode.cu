@@ -102,6 +102,7 @@ struct KParams {
     unsigned long long* done_count;   // step form: cells finished
     double t0, t1, rtol, atol;
     int max_steps, max_order, refine, steps;
+    int chunk;                        // persistent form: cells a warp claims per queue access
 };
 
 template <class MT>
@@ -163,16 +164,23 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
     const long long t_start = profiling ? clock64() : 0;
     unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long cell = gw;
+    unsigned long long next = 0;   // persistent form: next claimed cell and how many remain
+    int left = 0;
 #pragma unroll 1
     for (int iter = 0;; ++iter) {
         if (step_form) {
             if (iter > 0 || cell >= p.ncells) break;
         } else {
-            unsigned long long c = 0;
-            if (lane == 0) c = atomicAdd(p.queue, 1ULL);
-            c = __shfl_sync(kFull, c, 0);
-            if (c >= (unsigned long long)p.ncells) break;
-            cell = (long long)c;
+            if (left == 0) {
+                unsigned long long c = 0;
+                if (lane == 0) c = atomicAdd(p.queue, (unsigned long long)p.chunk);
+                next = __shfl_sync(kFull, c, 0);
+                left = p.chunk;
+            }
+            if (next >= (unsigned long long)p.ncells) break;
+            cell = (long long)next;
+            ++next;
+            --left;
         }
         WarpGlobal<MT, LinT>* wg = wglob + (step_form ? cell : gw);
         unsigned char* rec = step_form ? p.records + cell * (long long)R::kBytes : nullptr;
@@ -506,6 +514,7 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
     p.max_steps = h->opt.max_steps;
     p.max_order = h->opt.max_order;
     p.refine = h->opt.refine;
+    p.chunk = std::max(1, std::min(h->opt.queue_chunk, 64));
 }
 
 b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {

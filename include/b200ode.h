@@ -67,7 +67,9 @@ typedef struct {
     int32_t persistent;       /* 1 = persistent kernel + device work queue; 0 = one launch per BDF step */
     int32_t warps_per_block;  /* 0 = from the autotuner / occupancy */
     int32_t blocks_per_sm;    /* 0 = from occupancy */
-    int32_t queue_chunk;      /* cells a warp takes from the work queue at once (0 = 1) */
+    int32_t queue_chunk;      /* persistent form: consecutive cells a warp claims per work-queue
+                                 access, 1..64 (0 = 1); larger chunks trade queue traffic for
+                                 tail balance.  Results do not depend on it. */
     int32_t use_graph;        /* one-launch-per-step form: capture the step launches in a CUDA graph */
     int32_t device;           /* CUDA device ordinal (-1 = current) */
     int32_t profile_phases;   /* 1 = accumulate per-phase device cycles into b200ode_stats */
@@ -95,7 +97,8 @@ typedef struct {
  * mixed precision, persistent kernel. */
 void b200ode_default_options(b200ode_options* opts);
 
-/* Create a handle for a mechanism ("gri30", "gri30.yaml", "h2o2", "h2o2.yaml").
+/* Create a handle for a mechanism compiled into the library: "gri30", "h2o2",
+ * "nDodecane_Reitz" (".yaml" suffix optional) or "h2_li_2004" (".xml" optional).
  * Replaces the per-batch set-up of CVodeIntegratorGPU::integrateBatch
  * (CVodeIntegratorGPU.cpp:44-100) and CVodeIntegrator::init's NSP check
  * (CVodeIntegrator.cpp:34-50).  opts may be NULL (defaults). */

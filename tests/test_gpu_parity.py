@@ -181,6 +181,13 @@ def test_deterministic_and_batch_independent():
         assert Tc[0] == T1[c] and np.array_equal(Yc[:, 0], Y1[:, c])
 
 
+def test_queue_chunk_does_not_change_results():
+    b = W.make("gri_bimodal", 300, seed=12)
+    T1, Y1, s1, _, _ = run_gpu(b, native.B200ODE_MIXED)
+    T2, Y2, s2, _, _ = run_gpu(b, native.B200ODE_MIXED, queue_chunk=7)
+    assert np.array_equal(T1, T2) and np.array_equal(Y1, Y2) and np.array_equal(s1, s2)
+
+
 def test_step_form_equals_persistent_form():
     """The plain one-launch-per-step form keeps the full per-cell state in HBM
     between launches, so it reproduces the persistent kernel bit for bit."""
