@@ -270,6 +270,27 @@ __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParam
         }
 }
 
+// Mixture specific enthalpy h = sum_k Y_k h_k(T) / W_k [J/kg] of each cell,
+// one thread per cell (the reads of Y[k][c] are coalesced across the warp).
+// The NASA-7 enthalpy polynomial is the one the RHS uses.
+template <class MT>
+__global__ void __launch_bounds__(256) k_enthalpy(long long n, const double* T, const double* Y, double* hmass) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const DevMech& M = mech<MT>();
+    const double t = T[c];
+    const double invT = 1.0 / t;
+    double acc = 0.0;
+#pragma unroll 1
+    for (int k = 0; k < MT::N; ++k) {
+        const double* a = M.nasa + 14 * k + ((t <= __ldg(M.tmid + k)) ? 0 : 7);
+        const double hRT = __ldg(a + 0) + t * (__ldg(a + 1) * 0.5 + t * (__ldg(a + 2) * (1.0 / 3.0) +
+                           t * (__ldg(a + 3) * 0.25 + __ldg(a + 4) * 0.2 * t))) + __ldg(a + 5) * invT;
+        acc += Y[(long long)k * n + c] * hRT * __ldg(M.inv_mw + k);
+    }
+    hmass[c] = acc * kRU * t;
+}
+
 // FP64 FMA throughput probe: independent DFMA chains per thread.
 __global__ void k_fp64_peak(double* out, int iters) {
     double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9, a4 = a0 + 4e-9,
@@ -848,6 +869,41 @@ static b200ode_status eval_chem(b200ode_handle* h, int64_t n, const double* P, d
     cudaFreeAsync(d_out, st);
     CUDA_TRY(cudaStreamSynchronize(st));
     return rc;
+}
+
+b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n, const double* dT, const double* dY,
+                                            double* dh, void* stream) {
+    b200ode_status rc = check_args(h, n, 0.0, 0.0);
+    if (rc != B200ODE_OK) return rc;
+    if (n == 0) return B200ODE_OK;
+    if (!dT || !dY || !dh) return fail(B200ODE_ERR_INVALID, "null buffer");
+    NvtxRange range("b200ode_eval_enthalpy");
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    cudaStream_t st = (cudaStream_t)stream;
+    dispatch_mech(h, [&](auto mt, auto) {
+        k_enthalpy<decltype(mt)><<<blocks, 256, 0, st>>>(n, dT, dY, dh);
+        return B200ODE_OK;
+    });
+    CUDA_TRY(cudaGetLastError());
+    return B200ODE_OK;
+}
+
+b200ode_status b200ode_eval_enthalpy(b200ode_handle* h, int64_t n, const double* T, const double* Y, double* hmass) {
+    b200ode_status rc = check_args(h, n, 0.0, 0.0);
+    if (rc != B200ODE_OK) return rc;
+    if (n == 0) return B200ODE_OK;
+    if (!T || !Y || !hmass) return fail(B200ODE_ERR_INVALID, "null buffer");
+    rc = ensure_cap(h, (size_t)n);
+    if (rc != B200ODE_OK) return rc;
+    cudaStream_t st = h->stream;
+    const size_t nsp = h->hm.nsp;
+    CUDA_TRY(cudaMemcpyAsync(h->d_T, T, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(h->d_Y, Y, n * nsp * sizeof(double), cudaMemcpyHostToDevice, st));
+    rc = b200ode_eval_enthalpy_device(h, n, h->d_T, h->d_Y, h->d_P, st);   // d_P as the output scratch
+    if (rc != B200ODE_OK) return rc;
+    CUDA_TRY(cudaMemcpyAsync(hmass, h->d_P, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return B200ODE_OK;
 }
 
 b200ode_status b200ode_eval_rhs(b200ode_handle* h, int64_t n, const double* P, double Ps, const double* T,

@@ -8,6 +8,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "b200ode_integrator.hpp"
 
@@ -55,9 +56,15 @@ int cfg_int(const std::string& key, const std::string& v) {
 
 // Applies the b200 options of the config: precision (fp64 | mixed), refine (0 | 1),
 // max_steps, max_order, form (persistent | step), graph (0 | 1), warps_per_block,
-// blocks_per_sm, device.  Unknown values throw std::runtime_error.
-void apply_config(const IntegratorConfig& c, b200ode_options* o) {
+// blocks_per_sm, device, enthalpy (keep | update).  Unknown values throw
+// std::runtime_error.
+void apply_config(const IntegratorConfig& c, b200ode_options* o, bool* update_enthalpy) {
     std::string v;
+    if (cfg_get(c, "enthalpy", &v)) {
+        if (v == "keep") *update_enthalpy = false;
+        else if (v == "update") *update_enthalpy = true;
+        else throw std::runtime_error("b200.enthalpy must be keep or update, not '" + v + "'");
+    }
     if (cfg_get(c, "precision", &v)) {
         if (v == "fp64") o->precision = B200ODE_FP64;
         else if (v == "mixed") o->precision = B200ODE_MIXED;
@@ -93,7 +100,7 @@ void B200BDFIntegrator::init(std::shared_ptr<Context> c, IntegratorConfig config
     handle_ = nullptr;
     b200ode_options o = opts_;
     try {
-        apply_config(config, &o);
+        apply_config(config, &o, &update_enthalpy_);
     } catch (const std::exception& e) {
         logger->error(e.what());
         throw;
@@ -136,6 +143,18 @@ void B200BDFIntegrator::integrate(double t0, double t) {
         Tw[i] = T_[i];
         double* y = mesh->getSpeciesPointer(i);
         for (int k = 0; k < nsp; ++k) y[k] = Y_[(size_t)k * n + i];
+    }
+    if (update_enthalpy_ && mesh->hasEnthalpy()) {
+        // ENTHA of the integrated state (the reference's CVODE integrators keep the old value)
+        std::vector<double> hm(n);
+        const b200ode_status rh = b200ode_eval_enthalpy(handle_, n, T_.data(), Y_.data(), hm.data());
+        if (rh != B200ODE_OK) {
+            const std::string msg = std::string("B200BDFIntegrator: ") + b200ode_last_error();
+            logger->error(msg);
+            throw std::runtime_error(msg);
+        }
+        double* H = mesh->getEnthalpyPointer();
+        for (int i = 0; i < n; ++i) H[i] = hm[i];
     }
     if (stats_.n_failed) {
         std::stringstream ss;

@@ -27,7 +27,8 @@ EXPORTED = ["b200ode_default_options", "b200ode_create", "b200ode_destroy", "b20
             "b200ode_mechanism_species",
             "b200ode_integrate", "b200ode_integrate_device", "b200ode_integrate_device_noalloc",
             "b200ode_eval_rhs",
-            "b200ode_eval_jacobian", "b200ode_autotune", "b200ode_fp64_peak",
+            "b200ode_eval_jacobian", "b200ode_eval_enthalpy", "b200ode_eval_enthalpy_device",
+            "b200ode_autotune", "b200ode_fp64_peak",
             "b200ode_default_server_options", "b200ode_server_create", "b200ode_server_destroy",
             "b200ode_submit", "b200ode_poll", "b200ode_server_get_report",
             "b200ode_last_error", "b200ode_version"]
@@ -119,6 +120,11 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.b200ode_eval_rhs.restype = C.c_int
     lib.b200ode_eval_jacobian.argtypes = [C.c_void_p, C.c_int64, _dp, C.c_double, _dp, _dp, _dp]
     lib.b200ode_eval_jacobian.restype = C.c_int
+    lib.b200ode_eval_enthalpy.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp]
+    lib.b200ode_eval_enthalpy.restype = C.c_int
+    lib.b200ode_eval_enthalpy_device.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p]
+    lib.b200ode_eval_enthalpy_device.restype = C.c_int
     lib.b200ode_autotune.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
                                      C.c_double, C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
     lib.b200ode_autotune.restype = C.c_int
@@ -225,6 +231,15 @@ class Solver:
         dY = np.zeros((self.nsp - 1, n))
         _check(self.lib.b200ode_eval_rhs(self.h, n, _ptr(parr), ps, _ptr(T), _ptr(Y), _ptr(dT), _ptr(dY)))
         return dT, dY
+
+    def eval_enthalpy(self, T: np.ndarray, Y: np.ndarray) -> np.ndarray:
+        """Mixture specific enthalpy [J/kg] of cells (T[n], Y[nsp, n])."""
+        n = T.size
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        Y = np.ascontiguousarray(Y, dtype=np.float64)
+        out = np.zeros(n)
+        _check(self.lib.b200ode_eval_enthalpy(self.h, n, _ptr(T), _ptr(Y), _ptr(out)))
+        return out
 
     def eval_jacobian(self, T: np.ndarray, Y: np.ndarray, P) -> np.ndarray:
         """Analytic Jacobians [n, nsp, nsp] with J[c, i, j] = d f_i / d y_j (reference order)."""

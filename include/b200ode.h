@@ -189,6 +189,18 @@ b200ode_status b200ode_eval_rhs(b200ode_handle* h, int64_t n_cells, const double
 b200ode_status b200ode_eval_jacobian(b200ode_handle* h, int64_t n_cells, const double* P,
                                      double P_scalar, const double* T, const double* Y, double* jac);
 
+/* Mixture specific enthalpy [J/kg] of each cell from T (n_cells) and Y
+ * (nsp x n_cells, SoA, all species): h = sum_k Y_k h_k(T) / W_k with the
+ * mechanism's NASA-7 polynomials (host buffers; _device: device buffers, async
+ * on stream).  The reference's CVODE integrators leave the Mesh's ENTHA as it
+ * was; its Cantera integrator writes it after integrating
+ * (src/Integrators/CanteraIntegrator.cpp:93).  This gives the CVODE-semantics
+ * path an enthalpy consistent with the integrated state. */
+b200ode_status b200ode_eval_enthalpy(b200ode_handle* h, int64_t n_cells, const double* T, const double* Y,
+                                     double* h_mass);
+b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n_cells, const double* d_T,
+                                            const double* d_Y, double* d_h_mass, void* stream);
+
 /* Autotuner: integrates a sample of the given cells (the first min(n_cells,
  * 8192); device buffers as b200ode_integrate_device, left unmodified) with the
  * persistent kernel under each launch shape -- 4, 2 or 1 warps (cells) per CTA,

@@ -10,7 +10,8 @@
 //             [T, Y_0 .. Y_{nsp-2}], reltol/abstol from the config, 10000 steps at
 //             most, the config's pressure; on return the mesh holds the new T
 //             and Y with Y_{nsp-1} = 1 - sum(Y_0 .. Y_{nsp-2}); ENTHA is not
-//             touched (as in the CVODE integrators);
+//             touched (as in the CVODE integrators) unless the config says
+//             b200.enthalpy: update, which writes the enthalpy of the new state;
 //   clean     releases the device handle.
 // Differences: per-cell failures do not throw; the count is logged and the
 // per-cell CVODE status is kept (cellStatus()).  CUDA and allocation errors
@@ -52,4 +53,5 @@ private:
     std::vector<double> T_, Y_;   // SoA staging: T[n], Y[k * n + i]
     std::vector<int32_t> status_;
     b200ode_stats stats_;
+    bool update_enthalpy_ = false;   // config b200.enthalpy: update
 };

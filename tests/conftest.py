@@ -33,3 +33,9 @@ def golden_e2e():
 def y_ok(Y_test, Y_ref, rel=1e-4, abs_=1e-10):
     """Per-entry mass-fraction gate: |dY| <= max(rel*|Y_ref|, abs_)."""
     return np.abs(Y_test - Y_ref) <= np.maximum(rel * np.abs(Y_ref), abs_)
+
+
+@pytest.fixture(scope="session")
+def golden_enthalpy():
+    return dict(np.load(os.path.join(GOLDEN, "enthalpy_ref.npz")))
+

@@ -5,7 +5,8 @@
 //
 //   integrator_driver <type> <mechanism> <in.bin> <out.bin> [b200.key=value ...]
 // in.bin:  int32 n, int32 nsp, double dt, double pressure, double T[n], double Y[n][nsp]
-// out.bin: the same layout after integration, then int32 status[n]
+// out.bin: the same layout after integration, then int32 status[n], then
+//          double enthalpy[n] (every point is created with enthalpy 0)
 // Exit 0 on success; on an exception prints "EXCEPTION: <what>" and exits 3.
 #include <cstdint>
 #include <cstdio>
@@ -36,7 +37,7 @@ int main(int argc, char** argv) {
 
         auto mesh = std::make_shared<Mesh>();
         for (int i = 0; i < n; ++i)
-            mesh->addPoint(Point(nsp).setTemperature(T[i]).setSpecies(
+            mesh->addPoint(Point(nsp).setTemperature(T[i]).setEnthalpy(0.0).setSpecies(
                 std::vector<double>(Y.begin() + (size_t)i * nsp, Y.begin() + (size_t)(i + 1) * nsp)));
         auto logger = std::make_shared<MemoryLogger>();
         auto ctx = std::make_shared<Context>(logger, mesh);
@@ -62,6 +63,7 @@ int main(int argc, char** argv) {
         for (int i = 0; i < n; ++i)
             out.write(reinterpret_cast<const char*>(mesh->getSpeciesPointer(i)), 8 * (std::streamsize)nsp);
         out.write(reinterpret_cast<const char*>(status.data()), 4 * (std::streamsize)n);
+        out.write(reinterpret_cast<const char*>(mesh->getEnthalpyPointer()), 8 * (std::streamsize)n);
         return out ? 0 : 4;
     } catch (const std::exception& e) {
         std::cout << "EXCEPTION: " << e.what() << std::endl;

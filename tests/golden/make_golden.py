@@ -11,7 +11,13 @@ Writes:
                          ``eval_jacob`` (src/Mechanism/CPU/jacob.c:3) outputs;
   e2e_gri100.npz         the reference's 99-cell E2E input
                          (tests/Integrators/data/res_gri_100.csv) and its serial
-                         CVODE output (E2Etests/100/results_serial100.csv).
+                         CVODE output (E2Etests/100/results_serial100.csv);
+  enthalpy_ref.npz       states with the mixture enthalpy the reference's data
+                         files carry (ENTHA, computed by Cantera): every 50th
+                         row of ref_data/res_h2.csv (h2_li_2004) and the 99 rows
+                         of tests/Integrators/data/res_gri_100.csv (gri30).
+
+``python tests/golden/make_golden.py REF_DIR --only enthalpy`` writes only the last.
 The fixtures are small and committed; the GPU box never reads the reference.
 """
 from __future__ import annotations
@@ -68,5 +74,21 @@ def main(ref_dir: str):
     print("wrote", os.listdir(HERE))
 
 
+def enthalpy_fixture(ref_dir: str):
+    h2 = np.genfromtxt(os.path.join(ref_dir, "ref_data/res_h2.csv"), delimiter=",", names=True)[::50]
+    gri = np.loadtxt(os.path.join(ref_dir, "tests/Integrators/data/res_gri_100.csv"), delimiter=",", skiprows=1)
+    np.savez_compressed(
+        os.path.join(HERE, "enthalpy_ref.npz"),
+        h2_T=h2["TEMPE"], h2_Y=np.stack([h2[f"CO{k}"] for k in range(9)]), h2_h=h2["ENTHA"],
+        gri_T=gri[:, 54], gri_Y=np.ascontiguousarray(gri[:, 0:53].T), gri_h=gri[:, 53])
+    print("wrote enthalpy_ref.npz")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    args = [a for a in sys.argv[1:] if not a.startswith("--") and a != "enthalpy"]
+    ref = args[0] if args else "/root/reference"
+    if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "enthalpy":
+        enthalpy_fixture(ref)
+    else:
+        main(ref)
+        enthalpy_fixture(ref)

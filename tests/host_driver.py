@@ -38,5 +38,6 @@ def run(exe, tmpdir, itype, mech, T, Y_rows, dt, P, options=()):
     off = 24
     To = np.frombuffer(raw, np.float64, n, off); off += 8 * n
     Yo = np.frombuffer(raw, np.float64, n * nsp, off).reshape(n, nsp); off += 8 * n * nsp
-    st = np.frombuffer(raw, np.int32, n, off)
+    st = np.frombuffer(raw, np.int32, n, off); off += 4 * n
+    run.enthalpy = np.frombuffer(raw, np.float64, n, off).copy()
     return 0, r.stdout, To.copy(), Yo.copy(), st.copy()
