@@ -1,5 +1,5 @@
-"""The C-ABI library loads and exports every symbol include/b200ode.h declares
-(no compute calls: this runs without a GPU)."""
+"""The C-ABI libraries load and export every symbol include/b200ode.h and
+include/b200ode_io.h declare (no compute calls: this runs without a GPU)."""
 import ctypes
 import os
 import re
@@ -23,6 +23,16 @@ def test_library_exports_every_declared_symbol():
     missing = [s for s in syms if not hasattr(lib, s)]
     assert not missing, missing
     assert sorted(native.EXPORTED) == syms
+
+
+def test_host_library_exports_the_io_symbols():
+    build.build()
+    from hpc_ode_b200 import io
+    lib = ctypes.CDLL(io.HOST_LIB_PATH)
+    syms = declared_symbols("b200ode_io.h")
+    assert "b200ode_csv_read" in syms
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
 
 
 def test_loader_fails_loudly_without_library(tmp_path):
