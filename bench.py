@@ -40,6 +40,10 @@ L2_FLUSH_BYTES = 256 << 20
 # dram__bytes_write.sum, 8,192-cell GRI capture, mixed precision): the traffic
 # is the compulsory T/P/Y in + T/Y/status out, so it scales with the cell count.
 NCU_DRAM_BYTES_PER_CELL = {"gri30": 856.0}
+# Warp instructions per cell of the same capture (smsp__inst_executed.sum / cells,
+# 8,192 GRI cells, mixed): the kernel is bound by instruction issue latency, so
+# issued instructions against the SMs' peak issue rate is its telling roofline.
+NCU_WARP_INSTR_PER_CELL = {("gri30", "mixed"): 3.267e6}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -390,6 +394,17 @@ def main():
                 "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
                 "note": "compute-bound path (FP64 CUDA-core pipe); HBM fraction shown for the "
                         "contract, see fp64 block and profiles/"}
+    issue = None
+    ipc = NCU_WARP_INSTR_PER_CELL.get((batch.mech, args.precision))
+    if ipc:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        peak_issue = 4 * sms * mhz * 1e6            # one warp instruction per scheduler per cycle
+        ach = ipc * n / (kernel_ms * 1e-3)
+        issue = {"achieved_warp_inst_per_s": ach, "peak_warp_inst_per_s": peak_issue, "frac": ach / peak_issue,
+                 "source": "warp instructions per cell from ncu smsp__inst_executed.sum "
+                           "(profiles/k_bdf_gri8k_mixed_full.txt) x cells / CUDA-event kernel time; peak = "
+                           "4 schedulers x SMs x median SM clock"}
     fp64 = None
     try:
         pk = native.fp64_peak_gflops(dev.index)
@@ -465,6 +480,7 @@ def main():
         "e2e": e2e,
         "gpu_launches": args.steps * int(st["gpu_launches"]),
         "roofline": roofline,
+        "issue_roofline": issue,
         "fp64": fp64,
         "cpu_baseline": cpu,
         "fp64_step_form": fp64_step,
