@@ -184,15 +184,17 @@ def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample
             "oracle_failed": int((st_true["status"] != 0).sum())}
 
 
-def serving_block(native, device: int, n_requests: int, load: float, seed: int = 4) -> dict:
+def serving_block(native, device: int, n_requests: int, load: float, seed: int = 4,
+                  chunk_cells: int = 32768) -> dict:
     """Serving loop under Poisson arrivals: requests of the serving workload
     (log-uniform 1k-256k cells, 60 % H2 / 40 % GRI, dt in {1e-5, 1e-4}) are
     submitted at exponential inter-arrival times with rate load x the measured
     saturation request rate; latency is submit -> results in the caller's host
-    buffers (measured by the library's dispatcher thread)."""
+    buffers (measured by the library's dispatcher thread).  Requests larger
+    than chunk_cells run as consecutive launches of at most that many cells."""
     cal = list(W.serving_requests(12, seed=seed + 1))
     reqs = list(W.serving_requests(n_requests, seed=seed))
-    srv = native.Server(max_inflight=4, device=device)
+    srv = native.Server(max_inflight=4, device=device, chunk_cells=chunk_cells)
     try:
         # saturation: the calibration requests submitted at once (also warms handles and staging)
         t0 = time.perf_counter()
@@ -226,6 +228,7 @@ def serving_block(native, device: int, n_requests: int, load: float, seed: int =
                 "max_latency_ms": float(lat.max()), "mean_queue_ms": float(np.mean([i["queue_ms"] for i in infos])),
                 "cells_per_sec": cells / span, "cells": cells, "max_concurrent": rep["max_concurrent"],
                 "failed_cells": int(sum(i["n_failed"] for i in infos)),
+                "chunk_cells": chunk_cells,
                 "workload": "log-uniform 1k-256k cells, 60 % H2 (h2_1024 dists) / 40 % GRI (gri_32k dists), "
                             "dt in {1e-5, 1e-4} s, Poisson arrivals, host buffers"}
     finally:
@@ -267,6 +270,8 @@ def main():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--serving-requests", type=int, default=48)
     ap.add_argument("--serving-load", type=float, default=0.8)
+    ap.add_argument("--serving-chunk", type=int, default=32768,
+                    help="cells per launch of a serving request (larger requests run in chunks)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -445,7 +450,8 @@ def main():
     serving = None
     if rank == 0 and not args.no_serving:
         try:
-            serving = serving_block(native, dev.index, args.serving_requests, args.serving_load)
+            serving = serving_block(native, dev.index, args.serving_requests, args.serving_load,
+                                    chunk_cells=args.serving_chunk)
         except Exception as e:  # noqa: BLE001
             serving = {"error": str(e)}
 

@@ -8,12 +8,19 @@
 //      caller buffers, device range back to the arena, slot freed);
 //   2. admits queued requests while a slot (stream) is free and the request's
 //      footprint fits in the arena (first fit; FIFO with bounded backfill);
-//   3. for each admitted request: caller buffers -> pinned staging, one H2D
-//      copy of T|Y (+ P), the persistent BDF kernel, one D2H copy of
-//      T|Y|status and the call totals, an end event.
-// Device layout of a request's range (each part 256-byte aligned):
-//   T[n] | Y[nsp*n] | status[n] | P[n] (if per-cell) | ctl[16] | per-warp scratch
-// and the pinned staging buffer mirrors its first part (T|Y|status|P|totals).
+//   3. for each admitted request, chunk by chunk (at most chunk_cells cells
+//      each): caller buffers -> pinned staging, one H2D copy of T|Y (+ P), the
+//      persistent BDF kernel, one D2H copy of T|Y|status and the call totals,
+//      an end event.  The next chunk is launched only when the previous one has
+//      finished, so thread blocks of other requests take SMs in between: a
+//      256k-cell request no longer holds the whole GPU until it is done, and
+//      its device footprint is one chunk's.
+// Device layout of a request's range, sized for one chunk of m cells (each part
+// 256-byte aligned):
+//   T[m] | Y[nsp*m] | status[m] | P[m] (if per-cell) | ctl[16] | per-warp scratch
+// and the pinned staging buffer mirrors its first part (T|Y|status|P|totals);
+// staging gathers a chunk's cells out of the caller's n-cell arrays and
+// scatters the results back.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -72,7 +79,10 @@ struct Request {
     double* Y = nullptr;
     int32_t* status = nullptr;
     double t0 = 0.0, t1 = 0.0;
-    Layout lay;
+    Layout lay;              // one chunk's layout (chunk cells)
+    int64_t chunk = 0;       // cells per chunk
+    int64_t next_c0 = 0;     // first cell of the chunk in flight
+    int64_t cur_m = 0;       // cells of the chunk in flight
     size_t offset = 0;
     int slot = -1;
     int bypassed = 0;
@@ -129,6 +139,8 @@ struct b200ode_server {
     void run();
     bool admit_one(std::unique_lock<std::mutex>& lk);
     void start_request(Slot& s, Request* r);
+    bool launch_chunk(Slot& s, Request* r);
+    bool retire_chunk(Slot& s, Request* r);
     void finish_request(Slot& s, Request* r, cudaError_t e);
 };
 
@@ -167,40 +179,75 @@ struct ServerDeviceGuard {
 
 }  // namespace
 
-// Copies the request's inputs to pinned staging and enqueues copies + kernel on
-// the slot's stream.  Runs on the dispatcher thread without the lock: an
-// admitted request belongs to the dispatcher until it is marked done.
+// Starts a request: its first chunk.  Runs on the dispatcher thread without
+// the lock: an admitted request belongs to the dispatcher until it is done.
 void b200ode_server::start_request(Slot& s, Request* r) {
+    r->next_c0 = 0;
+    launch_chunk(s, r);   // on failure the request is already finished
+}
+
+// Stages cells [next_c0, next_c0 + m) and enqueues copies + kernel + end
+// event on the slot's stream.  Returns false (the request finished with an
+// error) if anything failed.
+bool b200ode_server::launch_chunk(Slot& s, Request* r) {
     const Layout& L = r->lay;
     unsigned char* d = base + r->offset;
-    auto fail_now = [&](cudaError_t e, const char* what) { finish_request(s, r, e ? e : cudaErrorUnknown), (void)what; };
+    const int64_t c0 = r->next_c0, m = std::min<int64_t>(r->chunk, r->n - c0);
+    r->cur_m = m;
+    auto fail_now = [&](cudaError_t e) {
+        finish_request(s, r, e ? e : cudaErrorUnknown);
+        return false;
+    };
     cudaError_t e = ensure_pinned(s, L.ctl + b200::kCtlWords * sizeof(unsigned long long));
-    if (e != cudaSuccess) return fail_now(e, "pinned staging");
-    const size_t n = (size_t)r->n;
-    std::memcpy(s.pinned + L.T, r->T, n * sizeof(double));
-    std::memcpy(s.pinned + L.Y, r->Y, n * r->nsp * sizeof(double));
-    if (r->P) std::memcpy(s.pinned + L.P, r->P, n * sizeof(double));
-    e = cudaEventRecord(s.ev_start, s.stream);
+    if (e != cudaSuccess) return fail_now(e);
+    // chunk SoA in staging (stride m), the layout the kernel sees for m cells
+    std::memcpy(s.pinned + L.T, r->T + c0, m * sizeof(double));
+    for (int k = 0; k < r->nsp; ++k)
+        std::memcpy(s.pinned + L.Y + (size_t)k * m * sizeof(double), r->Y + (size_t)k * r->n + c0, m * sizeof(double));
+    if (r->P) std::memcpy(s.pinned + L.P, r->P + c0, m * sizeof(double));
+    if (c0 == 0) e = cudaEventRecord(s.ev_start, s.stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d, s.pinned, L.in_bytes, cudaMemcpyHostToDevice, s.stream);
     if (e == cudaSuccess && r->P)
-        e = cudaMemcpyAsync(d + L.P, s.pinned + L.P, n * sizeof(double), cudaMemcpyHostToDevice, s.stream);
-    if (e != cudaSuccess) return fail_now(e, "H2D");
+        e = cudaMemcpyAsync(d + L.P, s.pinned + L.P, m * sizeof(double), cudaMemcpyHostToDevice, s.stream);
+    if (e != cudaSuccess) return fail_now(e);
     auto* ctl = reinterpret_cast<unsigned long long*>(d + L.ctl);
     b200ode_status rc = b200::launch_persistent(
-        r->h, r->n, r->P ? reinterpret_cast<const double*>(d + L.P) : nullptr, r->P_scalar,
+        r->h, m, r->P ? reinterpret_cast<const double*>(d + L.P) : nullptr, r->P_scalar,
         reinterpret_cast<double*>(d + L.T), reinterpret_cast<double*>(d + L.Y),
         reinterpret_cast<int32_t*>(d + L.status), r->t0, r->t1, ctl, d + L.wg, s.stream);
     if (rc != B200ODE_OK) {
         r->rc = rc;
         r->err = b200ode_last_error();
-        return finish_request(s, r, cudaSuccess);
+        finish_request(s, r, cudaSuccess);
+        return false;
     }
     e = cudaMemcpyAsync(s.pinned, d, L.out_bytes, cudaMemcpyDeviceToHost, s.stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s.pinned + L.ctl, ctl, b200::kCtlWords * sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, s.stream);
     if (e == cudaSuccess) e = cudaEventRecord(s.ev_end, s.stream);
-    if (e != cudaSuccess) return fail_now(e, "D2H");
+    if (e != cudaSuccess) return fail_now(e);
+    return true;
+}
+
+// The chunk in flight has finished: results to the caller's buffers, totals
+// accumulated; launches the next chunk.  Returns true when the request is
+// complete.
+bool b200ode_server::retire_chunk(Slot& s, Request* r) {
+    const Layout& L = r->lay;
+    const int64_t c0 = r->next_c0, m = r->cur_m;
+    std::memcpy(r->T + c0, s.pinned + L.T, m * sizeof(double));
+    for (int k = 0; k < r->nsp; ++k)
+        std::memcpy(r->Y + (size_t)k * r->n + c0, s.pinned + L.Y + (size_t)k * m * sizeof(double), m * sizeof(double));
+    if (r->status) std::memcpy(r->status + c0, s.pinned + L.status, m * sizeof(int32_t));
+    const auto* tot = reinterpret_cast<const unsigned long long*>(s.pinned + L.ctl) + 1;
+    r->info.total_nst += (int64_t)tot[0];
+    r->info.total_nni += (int64_t)tot[4];
+    r->info.n_failed += (int64_t)tot[7];
+    r->next_c0 = c0 + m;
+    if (r->next_c0 >= r->n) return true;
+    launch_chunk(s, r);   // on failure the request is already finished
+    return false;
 }
 
 // Completes a request: results to the caller (when the GPU side succeeded),
@@ -213,16 +260,7 @@ void b200ode_server::finish_request(Slot& s, Request* r, cudaError_t e) {
         r->err = std::string("request ") + std::to_string(r->id) + ": " + cudaGetErrorString(e);
     }
     if (r->rc == B200ODE_OK) {
-        const Layout& L = r->lay;
-        const size_t n = (size_t)r->n;
-        std::memcpy(r->T, s.pinned + L.T, n * sizeof(double));
-        std::memcpy(r->Y, s.pinned + L.Y, n * r->nsp * sizeof(double));
-        if (r->status) std::memcpy(r->status, s.pinned + L.status, n * sizeof(int32_t));
-        const auto* tot = reinterpret_cast<const unsigned long long*>(s.pinned + L.ctl) + 1;
-        r->info.total_nst = (int64_t)tot[0];
-        r->info.total_nni = (int64_t)tot[4];
-        r->info.n_failed = (int64_t)tot[7];
-        float ms = 0.f;
+        float ms = 0.f;   // first chunk's start to last chunk's end
         if (cudaEventElapsedTime(&ms, s.ev_start, s.ev_end) == cudaSuccess) r->info.device_ms = ms;
     }
     const Clock::time_point now = Clock::now();
@@ -293,7 +331,11 @@ void b200ode_server::run() {
         }
         if (!finished.empty()) {
             lk.unlock();
-            for (auto& f : finished) finish_request(*f.first, f.first->req, f.second);
+            for (auto& f : finished) {
+                Request* r = f.first->req;
+                if (f.second != cudaSuccess) finish_request(*f.first, r, f.second);
+                else if (retire_chunk(*f.first, r)) finish_request(*f.first, r, cudaSuccess);
+            }
             lk.lock();
         }
         // 2. admit
@@ -320,6 +362,7 @@ void b200ode_default_server_options(b200ode_server_options* o) {
     o->hbm_budget_bytes = 0;
     o->max_inflight = 4;
     o->max_queued = 4096;
+    o->chunk_cells = 32768;
 }
 
 b200ode_status b200ode_server_create(const b200ode_server_options* opts, b200ode_server** out) {
@@ -330,6 +373,7 @@ b200ode_status b200ode_server_create(const b200ode_server_options* opts, b200ode
     if (opts) o = *opts;
     if (o.max_inflight <= 0) o.max_inflight = 4;
     if (o.max_queued <= 0) o.max_queued = 4096;
+    if (o.chunk_cells <= 0) o.chunk_cells = 32768;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -412,10 +456,12 @@ b200ode_status b200ode_submit(b200ode_server* s, const char* mech_name, int64_t 
     b200ode_handle* h = it->second;
     const int nsp = b200ode_num_species(h);
     Layout lay;
+    int64_t chunk = 0;
     if (n > 0) {
-        const size_t wg = b200::persistent_scratch_bytes(h, n);
+        chunk = std::min<int64_t>(n, s->opt.chunk_cells);
+        const size_t wg = b200::persistent_scratch_bytes(h, chunk);
         if (wg == 0) return B200ODE_ERR_CUDA;
-        lay = Layout(n, nsp, P != nullptr, wg);
+        lay = Layout(chunk, nsp, P != nullptr, wg);
         if (lay.total > s->arena.capacity())
             return b200::set_error(B200ODE_ERR_INVALID, "request of " + std::to_string(n) + " cells needs " +
                                                             std::to_string(lay.total) +
@@ -424,6 +470,7 @@ b200ode_status b200ode_submit(b200ode_server* s, const char* mech_name, int64_t 
     }
     auto r = std::make_unique<Request>();
     r->lay = lay;
+    r->chunk = chunk;
     r->id = s->next_id++;
     r->h = h;
     r->nsp = nsp;

@@ -67,7 +67,7 @@ class Stats(C.Structure):
 
 class ServerOptions(C.Structure):
     _fields_ = [("solver", Options), ("hbm_budget_bytes", C.c_int64), ("max_inflight", C.c_int32),
-                ("max_queued", C.c_int32)]
+                ("max_queued", C.c_int32), ("chunk_cells", C.c_int32)]
 
 
 class RequestInfo(C.Structure):
@@ -292,7 +292,8 @@ class Server:
     """The request loop of the C ABI (b200ode_server_*): submit batches of cells,
     poll for their results; continuous batching on one GPU."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 4, max_queued: int = 4096, **solver_kw):
+    def __init__(self, hbm_budget_bytes: int = 0, max_inflight: int = 4, max_queued: int = 4096,
+                 chunk_cells: int = 32768, **solver_kw):
         self.lib = load()
         o = ServerOptions()
         self.lib.b200ode_default_server_options(C.byref(o))
@@ -303,6 +304,7 @@ class Server:
         o.hbm_budget_bytes = int(hbm_budget_bytes)
         o.max_inflight = int(max_inflight)
         o.max_queued = int(max_queued)
+        o.chunk_cells = int(chunk_cells)
         h = C.c_void_p()
         _check(self.lib.b200ode_server_create(C.byref(o), C.byref(h)))
         self.h = h

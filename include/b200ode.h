@@ -240,15 +240,20 @@ typedef struct {
     int64_t hbm_budget_bytes;   /* device bytes requests in flight may hold (0 = 25 % of free memory) */
     int32_t max_inflight;       /* requests on the GPU at once = streams (0 = 4) */
     int32_t max_queued;         /* requests waiting for admission before submit returns BUSY (0 = 4096) */
+    int32_t chunk_cells;        /* a request runs as consecutive launches of at most this many cells,
+                                   each launched when the previous one is done, so other requests'
+                                   blocks take SMs in between; its device footprint is one chunk's
+                                   (0 = 32768) */
 } b200ode_server_options;
 
 typedef struct {
     int64_t n_cells;
     int64_t n_failed;          /* cells whose status != B200ODE_CELL_SUCCESS */
     int64_t total_nst, total_nni;
-    int64_t footprint_bytes;   /* device bytes the request held while in flight */
+    int64_t footprint_bytes;   /* device bytes the request held while in flight (one chunk's) */
     double queue_ms;           /* submit -> admitted */
-    double device_ms;          /* H2D + kernel + D2H on its stream (CUDA events) */
+    double device_ms;          /* first chunk's H2D to last chunk's D2H on its stream (CUDA
+                                  events; includes the host gaps between chunks) */
     double latency_ms;         /* submit -> results in the caller's buffers */
 } b200ode_request_info;
 
@@ -269,7 +274,7 @@ void b200ode_server_destroy(b200ode_server* s);
  * cell_status (may be NULL) receive the results; P, T, Y and cell_status must
  * stay valid and untouched until b200ode_poll reports the request done.
  * Returns B200ODE_ERR_BUSY when max_queued requests wait, B200ODE_ERR_INVALID
- * when the request alone exceeds the server's device budget. */
+ * when one chunk of the request alone exceeds the server's device budget. */
 b200ode_status b200ode_submit(b200ode_server* s, const char* mech_name, int64_t n_cells, const double* P,
                               double P_scalar, double* T, double* Y, double t0, double t1,
                               int32_t* cell_status, uint64_t* request_id);

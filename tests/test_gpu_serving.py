@@ -105,6 +105,42 @@ def test_admission_by_device_footprint():
         srv.close()
 
 
+def test_chunked_request_matches_synchronous_path():
+    """A request larger than chunk_cells runs as consecutive launches (here
+    3 chunks of at most 512 cells, with small requests between them); its
+    results, statuses and summed step totals equal the synchronous call's, and
+    it holds one chunk's device footprint."""
+    big = _req("gri_32k", 1300, 70)
+    small = [_req("h2_1024", 100, 71 + i, dt=1e-5) for i in range(3)]
+    s = native.Solver(big.mech)
+    Ts, Ys = big.T.copy(), np.ascontiguousarray(big.Y.copy())
+    sts, stats, _ = s.integrate(Ts, Ys, big.P, big.dt)
+    s.close()
+    srv = native.Server(max_inflight=4, chunk_cells=512)
+    try:
+        rid, T, Y = _submit(srv, big)
+        subs = [_submit(srv, b) for b in small]
+        st, info = srv.poll(rid, -1)
+        assert np.array_equal(st, sts)
+        _same(T, Y, Ts, Ys)
+        assert info["n_cells"] == 1300 and info["n_failed"] == 0 and info["total_nst"] > 0
+        assert (info["total_nst"], info["total_nni"]) == (stats["total_nst"], stats["total_nni"])
+        for (r, Tb, Yb), b in zip(subs, small):
+            stb, _ = srv.poll(r, -1)
+            Tr, Yr, str_ = _sync(b)
+            assert np.array_equal(stb, str_)
+            _same(Tb, Yb, Tr, Yr)
+    finally:
+        srv.close()
+    one = native.Server(max_inflight=1, chunk_cells=512)
+    try:
+        rid, _, _ = _submit(one, _req("gri_32k", 512, 79))
+        _, info512 = one.poll(rid, -1)
+    finally:
+        one.close()
+    assert info["footprint_bytes"] == info512["footprint_bytes"]
+
+
 def test_stream_of_small_requests_reports_latency():
     rng = np.random.default_rng(7)
     srv = native.Server(max_inflight=4)
