@@ -28,6 +28,7 @@
 #include "mech/h2o2_mech.h"
 #include "mech/nDodecane_Reitz_mech.h"
 #include "mech/h2_li_2004_mech.h"
+#include "mech/ESTiMatE-Mech_04042022_mech.h"
 
 using namespace b200;
 
@@ -57,19 +58,27 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
     } while (0)
 
 #define GEN_TABLES(tag, PFX)                                                                         \
-    GenTables{#tag, PFX##_NSP, PFX##_NRXN, PFX##_MAXP, PFX##_NTB, tag##_species_names, tag##_mw,      \
+    GenTables{#tag, PFX##_NSP, PFX##_NRXN, PFX##_MAXP, PFX##_NTB, PFX##_NU_DEN, PFX##_NPLOGLEV,       \
+              PFX##_NPLOGTERM, tag##_species_names, tag##_mw,                                         \
               tag##_tmid, tag##_nasa_lo, tag##_nasa_hi, tag##_rxn_type, tag##_rxn_rev, tag##_rxn_A,   \
               tag##_rxn_logA, tag##_rxn_b, tag##_rxn_EaR, tag##_rxn_A0, tag##_rxn_logA0, tag##_rxn_b0, \
               tag##_rxn_EaR0, tag##_rxn_troe, tag##_rxn_troe_T2, tag##_rxn_reac_sp,                   \
               tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp,  \
-              tag##_tb_alpha}
+              tag##_tb_alpha, tag##_plog_off, tag##_plog_lnP, tag##_plog_term_off, tag##_plog_A,      \
+              tag##_plog_logA, tag##_plog_b, tag##_plog_EaR}
 
-enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3 };
+enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3, MECH_ESTIMATE = 4 };
 
-using GriT = MechT<MECH_GRI30_NSP, MECH_GRI30_NRXN, MECH_GRI30>;
-using H2T = MechT<MECH_H2O2_NSP, MECH_H2O2_NRXN, MECH_H2O2>;
-using NdT = MechT<MECH_NDODECANE_REITZ_NSP, MECH_NDODECANE_REITZ_NRXN, MECH_NDODECANE>;
-using H2LiT = MechT<MECH_H2_LI_2004_NSP, MECH_H2_LI_2004_NRXN, MECH_H2LI>;
+#define MECH_TRAITS(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG>
+using GriT = MECH_TRAITS(MECH_GRI30, MECH_GRI30);
+using H2T = MECH_TRAITS(MECH_H2O2, MECH_H2O2);
+using NdT = MECH_TRAITS(MECH_NDODECANE_REITZ, MECH_NDODECANE);
+using H2LiT = MECH_TRAITS(MECH_H2_LI_2004, MECH_H2LI);
+// kerosene (214 species): mixed precision only -- one warp's FP32 Newton
+// matrix (214 x 215 x 4 B = 184 KB) fills an SM's shared memory; the FP64
+// matrix would not fit
+using EstT = MECH_TRAITS(MECH_ESTIMATE_MECH_04042022, MECH_ESTIMATE);
+static_assert(MECH_ESTIMATE + 1 == kNumMech, "one descriptor per mechanism");
 
 int mech_from_name(const char* name) {
     if (!name) return -1;
@@ -80,7 +89,19 @@ int mech_from_name(const char* name) {
     if (s == "h2o2") return MECH_H2O2;
     if (s == "nDodecane_Reitz") return MECH_NDODECANE;
     if (s == "h2_li_2004") return MECH_H2LI;
+    if (s == "ESTiMatE-Mech_04042022") return MECH_ESTIMATE;
     return -1;
+}
+
+int dispatch_units(int mech) {
+    switch (mech) {
+        case MECH_GRI30: return GriT::NUNITMAX;
+        case MECH_H2O2: return H2T::NUNITMAX;
+        case MECH_NDODECANE: return NdT::NUNITMAX;
+        case MECH_H2LI: return H2LiT::NUNITMAX;
+        case MECH_ESTIMATE: return EstT::NUNITMAX;
+        default: return 0;
+    }
 }
 
 }  // namespace
@@ -440,6 +461,7 @@ b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
     if (h->mech == MECH_GRI30) return fp64 ? f(GriT{}, double{}) : f(GriT{}, float{});
     if (h->mech == MECH_NDODECANE) return fp64 ? f(NdT{}, double{}) : f(NdT{}, float{});
     if (h->mech == MECH_H2LI) return fp64 ? f(H2LiT{}, double{}) : f(H2LiT{}, float{});
+    if (h->mech == MECH_ESTIMATE) return f(EstT{}, float{});   // FP64 refused at creation
     return fp64 ? f(H2T{}, double{}) : f(H2T{}, float{});
 }
 
@@ -635,6 +657,7 @@ int32_t b200ode_mechanism_species(const char* mech_name) {
         case MECH_H2O2: return MECH_H2O2_NSP;
         case MECH_NDODECANE: return MECH_NDODECANE_REITZ_NSP;
         case MECH_H2LI: return MECH_H2_LI_2004_NSP;
+        case MECH_ESTIMATE: return MECH_ESTIMATE_MECH_04042022_NSP;
         default: return -1;
     }
 }
@@ -646,7 +669,8 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     if (mech < 0)
         return fail(B200ODE_ERR_MECHANISM,
                     std::string("unknown mechanism '") + (mech_name ? mech_name : "(null)") +
-                        "' (available: gri30.yaml, h2o2.yaml, nDodecane_Reitz.yaml, h2_li_2004.xml)");
+                        "' (available: gri30.yaml, h2o2.yaml, nDodecane_Reitz.yaml, h2_li_2004.xml, "
+                        "ESTiMatE-Mech_04042022.xml)");
     b200ode_options o;
     b200ode_default_options(&o);
     if (opts) o = *opts;
@@ -656,6 +680,11 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     if (o.max_order < 1 || o.max_order > 5) o.max_order = 5;
     if (o.precision != B200ODE_FP64 && o.precision != B200ODE_MIXED)
         return fail(B200ODE_ERR_INVALID, "precision must be B200ODE_FP64 or B200ODE_MIXED");
+    if (mech == MECH_ESTIMATE && o.precision == B200ODE_FP64)
+        return fail(B200ODE_ERR_INVALID,
+                    "ESTiMatE-Mech_04042022 (214 unknowns) runs in B200ODE_MIXED only: its FP64 Newton "
+                    "matrix (" + std::to_string(sizeof(WarpSmem<EstT, double>)) +
+                        " bytes of shared memory per cell) exceeds an SM's shared memory");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -668,11 +697,19 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     h->hm = pack_mechanism(mech == MECH_GRI30  ? GEN_TABLES(gri30, MECH_GRI30)
                            : mech == MECH_H2O2 ? GEN_TABLES(h2o2, MECH_H2O2)
                            : mech == MECH_H2LI ? GEN_TABLES(h2_li_2004, MECH_H2_LI_2004)
+                           : mech == MECH_ESTIMATE ? GEN_TABLES(estimate_mech_04042022, MECH_ESTIMATE_MECH_04042022)
                                                : GEN_TABLES(ndodecane_reitz, MECH_NDODECANE_REITZ),
                            &err);
     if (h->hm.nsp == 0) {
         delete h;
         return fail(B200ODE_ERR_MECHANISM, "mechanism packing failed: " + err);
+    }
+    // the per-warp gather scratch is sized at compile time from the generated unit count
+    const int units_max = dispatch_units(mech);
+    if (h->hm.nunit > units_max) {
+        delete h;
+        return fail(B200ODE_ERR_MECHANISM, "mechanism packing: " + std::to_string(h->hm.nunit) +
+                                               " gather units, the kernels hold " + std::to_string(units_max));
     }
     auto cleanup = [&](b200ode_status st) { b200ode_destroy(h); return st; };
     if (o.device >= 0) {

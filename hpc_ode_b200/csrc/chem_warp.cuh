@@ -32,7 +32,12 @@ namespace b200 {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kRU = 8314.4621;
 
-template <int N_, int NR_, int ID_>
+// Compile-time shape of one generated mechanism: species count, reaction
+// count, descriptor index, the denominator of its stoichiometric coefficients
+// (1, or 2 / 4 with fractional product coefficients), its gather units and
+// whether it has PLOG reactions (the PLOG branch is compiled only then: the
+// reaction code is on the instruction-fetch-bound hot path).
+template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_>
 struct MechT {
     static constexpr int ID = ID_;                            // index into c_mech
     static constexpr int N = N_;                              // state length == species count
@@ -40,11 +45,14 @@ struct MechT {
     static constexpr int NSLOT = ((NR_ + 32) / 32) * 32;      // reaction slots (>= 1 padding slot)
     static constexpr int NG = NSLOT / 32;                     // reaction groups
     static constexpr int LDA = (N_ % 2 == 0) ? N_ + 1 : N_;   // odd stride: conflict-free rows/cols
-    static constexpr int NUNITMAX = N_ + (6 * NSLOT) / kGatherUnit + 1;   // gather units bound
+    static constexpr int NU_DEN = NU_DEN_;                    // gather words hold nu * NU_DEN
+    static constexpr int NUNITMAX = NUNITS_;                  // gather units (checked at creation)
+    static constexpr bool PLOG = NPLOG_ > 0;
 };
 
 // Mechanism descriptors (one per compiled mechanism), set once per device.
-__constant__ DevMech c_mech[4];
+constexpr int kNumMech = 5;
+__constant__ DevMech c_mech[kNumMech];
 
 template <class MT>
 __device__ __forceinline__ const DevMech& mech() { return c_mech[MT::ID]; }
@@ -139,6 +147,7 @@ struct CellThermo {
 // cache), so every call site that is not a full inline expansion helps.
 __device__ __noinline__ double ode_exp(double x) { return exp(x); }
 __device__ __noinline__ double ode_log10(double x) { return log10(x); }
+__device__ __noinline__ double ode_log(double x) { return log(x); }
 __device__ __noinline__ double ode_exp10(double x) { return exp10(x); }
 __device__ __noinline__ double ode_pow(double x, double y) { return pow(x, y); }
 // IEEE division out of line: an inline FP64 division is ~40 instructions, so
@@ -269,6 +278,49 @@ __device__ __noinline__ FallOut falloff(int s, int fl, double T, double logT, do
     return o;
 }
 
+// Pressure-dependent Arrhenius (PLOG) rate of slot s: ln k linear in ln P
+// between the two tabulated pressures that bracket the cell's P, the end
+// level's k outside the table (Cantera's PLOG definition, which the
+// reference's Cantera integrator evaluates for these reactions); a level's k
+// is the sum of its Arrhenius terms.  Returns ln k and d ln k / dT.
+struct PlogOut {
+    double lnk, dlnk_dT;
+};
+
+template <class MT>
+__device__ __noinline__ PlogOut plog_rate(int s, double T, double logT, double invT, double lnP) {
+    const DevMech& M = mech<MT>();
+    const int l0 = __ldg(M.plog_lev0 + s), l1 = l0 + __ldg(M.plog_nlev + s) - 1;
+    int lo = l0, hi = l0;
+    double w = 0.0;
+    if (lnP >= __ldg(M.plog_lnP + l1)) {
+        lo = hi = l1;
+    } else if (lnP > __ldg(M.plog_lnP + l0)) {
+        while (lo + 1 < l1 && __ldg(M.plog_lnP + lo + 1) < lnP) ++lo;
+        hi = lo + 1;
+        const double p0 = __ldg(M.plog_lnP + lo);
+        w = ode_div(lnP - p0, __ldg(M.plog_lnP + hi) - p0);
+    }
+    double lk[2], dl[2];
+#pragma unroll 1
+    for (int e = 0; e < 2; ++e) {
+        const int l = e ? hi : lo;
+        double k = 0.0, dk = 0.0;
+        const int t1 = __ldg(M.plog_toff + l + 1);
+#pragma unroll 1
+        for (int t = __ldg(M.plog_toff + l); t < t1; ++t) {
+            const double b = __ldg(M.plog_b + t), EaR = __ldg(M.plog_EaR + t);
+            const double kt = (b == 0.0 && EaR == 0.0) ? __ldg(M.plog_A + t)
+                                                       : ode_exp(__ldg(M.plog_logA + t) + b * logT - EaR * invT);
+            k += kt;
+            dk += kt * (b + EaR * invT) * invT;
+        }
+        lk[e] = ode_log(k);
+        dl[e] = ode_div(dk, k);
+    }
+    return PlogOut{(1.0 - w) * lk[0] + w * lk[1], (1.0 - w) * dl[0] + w * dl[1]};
+}
+
 // Cell quantities the reaction phase needs (passed by value to the
 // out-of-line slot evaluation).
 struct RxnCtx {
@@ -294,11 +346,18 @@ __device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, u
     constexpr int ns = MT::NSLOT;
     const int r0 = __ldg(M.rf + s), r1 = __ldg(M.rf + ns + s), r2 = __ldg(M.rf + 2 * ns + s);
     const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
-    const double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
+    double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
+    if (deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
+    if constexpr (MT::PLOG) {
+        if (fl & kFlagPlog) {   // P = m R T
+            const PlogOut pl = plog_rate<MT>(s, c.T, c.logT, c.invT, ode_log(c.m * kRU * c.T));
+            lkf = pl.lnk;
+            o.dlnkf_dT = pl.dlnk_dT;
+        }
+    }
     const double kf = (fl & kFlagConstK) ? __ldg(M.Aconst + s) : ode_exp(lkf);
     o.kf = kf;
     o.Rf = kf * ((C[r0] * C[r1]) * C[r2]);
-    if (deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
     if (fl & kFlagRev) {
         const int p0 = __ldg(M.pf + s), p1 = __ldg(M.pf + ns + s), p2 = __ldg(M.pf + 2 * ns + s);
         const int dnu = __ldg(M.dnu + s);
@@ -351,7 +410,9 @@ __device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off,
 #pragma unroll 2
     for (int e = 0; e < gmax; ++e) {
         const int w = __ldg(gw + 32 * e);
-        acc += (double)(((w >> 11) & 31) - 16) * src[w & 2047];
+        double nu = (double)(((w >> 11) & 31) - 16);
+        if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
+        acc += nu * src[w & 2047];
         const bool last = (w >> 16) & 1;
         if (last) sm->part[w >> 17] = acc;
         acc = last ? 0.0 : acc;
@@ -463,9 +524,9 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             if (fl & kFlagRev) {
                 double dH = 0.0;
 #pragma unroll
-                for (int e = 0; e < 6; ++e) {
+                for (int e = 0; e < kJRow; ++e) {
                     const int k = __ldg(M.jrow + e * ns + s);
-                    if (k >= 0) dH += (double)__ldg(M.jnu + e * ns + s) * sm->H[k];
+                    if (k >= 0) dH += __ldg(M.jnu + e * ns + s) * sm->H[k];
                 }
                 dlnkr = o.dlnkf_dT - (dH - (double)__ldg(M.dnu + s)) * c.invT;
             }
@@ -493,10 +554,10 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             const int off = __ldg(M.tb_off + s), len = __ldg(M.tb_len + s);
             const int cat = (fl & kFlagCatalyst) ? __ldg(M.cat_sp + s) : -1;
 #pragma unroll 1
-            for (int e = 0; e < 6; ++e) {
+            for (int e = 0; e < kJRow; ++e) {
                 const int k = __ldg(M.jrow + e * ns + s);
                 if (k < 0) break;
-                const double nu = (double)__ldg(M.jnu + e * ns + s);
+                const double nu = __ldg(M.jnu + e * ns + s);
                 LinT* row = A + k * LDA;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {

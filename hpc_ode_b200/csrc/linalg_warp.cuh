@@ -136,8 +136,16 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
             if (i < k) x[s] -= A[i * LDA + k] * xk;
         }
     }
+    // A species no reaction changes has a zero row in J, so its row of M is
+    // the identity row and its solution component is exactly its right-hand
+    // side; taking b itself keeps such species (inert colliders such as Ar,
+    // He) free of the round-off the pivoted LinT solve would give them.
+    const DevMech& M = mech<MT>();
 #pragma unroll
-    for (int s = 0; s < NS; ++s) out.v[s] = (double)x[s];
+    for (int s = 0; s < NS; ++s) {
+        const int i = lane + 32 * s;
+        out.v[s] = (i < N - 1 && __ldg(M.inert + i)) ? b[s] : (double)x[s];
+    }
     return out;
 }
 

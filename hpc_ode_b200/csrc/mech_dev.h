@@ -6,7 +6,8 @@
 // kernels read:
 //   * species arrays (molecular weights, NASA-7 coefficients), index k;
 //   * reaction "slots": reactions sorted by kind (elementary, third-body,
-//     catalyst third-body, Lindemann, Troe) and padded to groups of 32 so that
+//     catalyst third-body, Lindemann, Troe, pressure-dependent Arrhenius) and
+//     padded to groups of 32 so that
 //     the 32 lanes of a warp evaluate 32 reactions of one kind with the same
 //     instruction stream.  Every field is a separate array indexed by slot,
 //     so one group's load is one coalesced 32-wide access;
@@ -31,12 +32,17 @@ constexpr int kFlagActive = 1 << 4;  // real reaction (0 for padding slots)
 constexpr int kFlagT2 = 1 << 5;      // Troe with T2 term
 constexpr int kFlagConstK0 = 1 << 6; // k0 = A0
 constexpr int kFlagCatalyst = 1 << 7;  // third body is one species s: [M] = m - sum(C) + C_s
+constexpr int kFlagPlog = 1 << 8;    // pressure-dependent Arrhenius (type 0): kf from the PLOG tables
+
+// Species with nonzero net stoichiometry per reaction (rows of jrow / jnu).
+constexpr int kJRow = 8;
 
 // Balanced species gather: the (species, reaction) pairs are cut into units of
 // at most kGatherUnit entries, and units are dealt to the 32 lanes so each lane
 // sums about the same number of entries.  Entry word (int32):
-//   bits 0-10  reaction slot            bits 11-15 net stoichiometry + 16
+//   bits 0-10  reaction slot            bits 11-15 net stoichiometry x nu_den + 16
 //   bit  16    last entry of its unit   bits 17-31 unit index
+// (nu_den = 1, or 2 / 4 for mechanisms with fractional product coefficients).
 constexpr int kGatherUnit = 24;
 
 // Pointers into one device allocation (all arrays contiguous).
@@ -68,16 +74,27 @@ struct DevMech {
     const int* tb_len;      // [nslot]
     const int* tb_sp;       // [ntb]
     const double* tb_alpha; // [ntb]
-    const int* jrow;        // [6][nslot] species with nonzero net stoichiometry (-1 = none)
-    const int* jnu;         // [6][nslot] their net stoichiometric coefficient
+    const int* jrow;        // [kJRow][nslot] species with nonzero net stoichiometry (-1 = none)
+    const double* jnu;      // [kJRow][nslot] their net stoichiometric coefficient
     const int* sp_off;      // [nsp + 1]
     const int* sp_slot;     // [nent]
-    const int* sp_nu;       // [nent]
+    const int* sp_nu;       // [nent] net stoichiometry x nu_den
     const int* cat_sp;      // [nslot] catalyst species (or -1)
     int gmax;               // entries per lane in the balanced gather
     int nunit;              // gather units
     const int* gword;       // [gmax][32] entry words, lane innermost (coalesced)
     const int* unit_off;    // [nsp + 1] units of each species (contiguous, in order)
+    // PLOG slots: levels plog_lev0[s] .. plog_lev0[s] + plog_nlev[s] - 1 (ln P
+    // ascending); level l's Arrhenius terms plog_toff[l] .. plog_toff[l + 1] - 1
+    const int* plog_lev0;   // [nslot]
+    const int* plog_nlev;   // [nslot]
+    const double* plog_lnP; // [nlev]
+    const int* plog_toff;   // [nlev + 1]
+    const double* plog_A;   // [nterm]
+    const double* plog_logA;
+    const double* plog_b;
+    const double* plog_EaR;
+    const int* inert;       // [nsp] 1: no reaction changes species k (its rows of J are zero)
 };
 
 // Host image of DevMech: one byte buffer plus offsets, copied to the device once.
@@ -92,7 +109,8 @@ struct HostMech {
     size_t o_mw, o_inv_mw, o_tmid, o_nasa, o_logA, o_b, o_EaR, o_Aconst, o_lnPfac, o_logA0, o_b0,
         o_EaR0, o_A0const, o_troe_a, o_troe_iT3, o_troe_iT1, o_troe_T2, o_flags, o_rf, o_pf,
         o_dnu, o_tb_off, o_tb_len, o_tb_sp, o_tb_alpha, o_jrow, o_jnu, o_sp_off, o_sp_slot,
-        o_sp_nu, o_cat_sp, o_gword, o_unit_off;
+        o_sp_nu, o_cat_sp, o_gword, o_unit_off, o_plog_lev0, o_plog_nlev, o_plog_lnP, o_plog_toff,
+        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert;
     int gmax = 0, nunit = 0;
 
     DevMech bind(const unsigned char* base) const {
@@ -124,7 +142,7 @@ struct HostMech {
         d.tb_sp = (const int*)(base + o_tb_sp);
         d.tb_alpha = (const double*)(base + o_tb_alpha);
         d.jrow = (const int*)(base + o_jrow);
-        d.jnu = (const int*)(base + o_jnu);
+        d.jnu = (const double*)(base + o_jnu);
         d.sp_off = (const int*)(base + o_sp_off);
         d.sp_slot = (const int*)(base + o_sp_slot);
         d.sp_nu = (const int*)(base + o_sp_nu);
@@ -133,6 +151,15 @@ struct HostMech {
         d.nunit = nunit;
         d.gword = (const int*)(base + o_gword);
         d.unit_off = (const int*)(base + o_unit_off);
+        d.plog_lev0 = (const int*)(base + o_plog_lev0);
+        d.plog_nlev = (const int*)(base + o_plog_nlev);
+        d.plog_lnP = (const double*)(base + o_plog_lnP);
+        d.plog_toff = (const int*)(base + o_plog_toff);
+        d.plog_A = (const double*)(base + o_plog_A);
+        d.plog_logA = (const double*)(base + o_plog_logA);
+        d.plog_b = (const double*)(base + o_plog_b);
+        d.plog_EaR = (const double*)(base + o_plog_EaR);
+        d.inert = (const int*)(base + o_inert);
         return d;
     }
 };
@@ -140,13 +167,19 @@ struct HostMech {
 // Raw generated tables of one mechanism (pointers to the static arrays).
 struct GenTables {
     const char* name;
-    int nsp, nrxn, maxp, ntb;
+    int nsp, nrxn, maxp, ntb, nu_den, nplog_lev, nplog_term;
     const char* const* species_names;
     const double *mw, *tmid, *nasa_lo, *nasa_hi;
     const int *type, *rev;
     const double *A, *logA, *b, *EaR, *A0, *logA0, *b0, *EaR0, *troe;
-    const int *troeT2, *reac_sp, *reac_nu, *prod_sp, *prod_nu, *tb_off, *tb_sp;
+    const int *troeT2, *reac_sp, *reac_nu, *prod_sp;
+    const double* prod_nu;   // fractional only in irreversible reactions (multiples of 1 / nu_den)
+    const int *tb_off, *tb_sp;
     const double* tb_alpha;
+    const int* plog_off;     // [nrxn + 1] level range of each reaction
+    const double* plog_lnP;
+    const int* plog_term_off;
+    const double *plog_A, *plog_logA, *plog_b, *plog_EaR;
 };
 
 // Build the packed image.  Returns an empty name on failure (message in err).
@@ -164,7 +197,13 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
         int tbl = g.tb_off[r + 1] - g.tb_off[r];
         if (t == 0) return g.rev[r] ? 1 : 0;
         if (t == 1) return tbl > 16 ? 3 : 2;
-        return 2 + t;   // 4 Lindemann, 5 Troe
+        return 2 + t;   // 4 Lindemann, 5 Troe, 6 PLOG
+    };
+    const int den = g.nu_den;
+    auto scaled = [&](double nu, int* out) {   // nu * nu_den as an exact integer
+        const double x = nu * den;
+        *out = (int)std::lround(x);
+        return std::fabs(x - *out) < 1e-9;
     };
     std::vector<int> order(nr);
     for (int r = 0; r < nr; ++r) order[r] = r;
@@ -177,22 +216,32 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
     std::vector<double> logA(ns, 0), b(ns, 0), EaR(ns, 0), Ac(ns, 0), lnPfac(ns, 0), logA0(ns, 0),
         b0(ns, 0), EaR0(ns, 0), A0c(ns, 0), ta(ns, 0), tiT3(ns, 0), tiT1(ns, 0), tT2(ns, 0);
     std::vector<int> flags(ns, 0), rf(3 * ns, n), pf(3 * ns, n), dnu(ns, 0), tboff(ns, 0),
-        tblen(ns, 0), jrow(6 * ns, -1), jnu(6 * ns, 0), catsp(ns, -1);
+        tblen(ns, 0), jrow(kJRow * ns, -1), catsp(ns, -1), plev0(ns, 0), pnlev(ns, 0);
+    std::vector<double> jnu(kJRow * ns, 0.0);
+    std::vector<int> jnu_scaled(kJRow * ns, 0);
     std::vector<int> tbsp;
     std::vector<double> tbal;
     const double lnPR = std::log(101325.0 / 8314.4621);
     for (int s = 0; s < ns; ++s) {
         int r = h.slot_rxn[s];
         if (r < 0) continue;
-        int fl = g.type[r] | kFlagActive;
+        const bool plog = g.type[r] == 4;
+        int fl = (plog ? 0 : g.type[r]) | kFlagActive;
         if (g.rev[r]) fl |= kFlagRev;
-        if (g.b[r] == 0.0 && g.EaR[r] == 0.0) fl |= kFlagConstK;
+        if (plog) {
+            fl |= kFlagPlog;
+            plev0[s] = g.plog_off[r];
+            pnlev[s] = g.plog_off[r + 1] - g.plog_off[r];
+            if (pnlev[s] < 1) { *err = "PLOG reaction without pressure levels"; return HostMech(); }
+        } else if (g.b[r] == 0.0 && g.EaR[r] == 0.0) {
+            fl |= kFlagConstK;
+        }
         if (g.b0[r] == 0.0 && g.EaR0[r] == 0.0) fl |= kFlagConstK0;
         if (g.troeT2[r]) fl |= kFlagT2;
         flags[s] = fl;
         logA[s] = g.logA[r]; b[s] = g.b[r]; EaR[s] = g.EaR[r]; Ac[s] = g.A[r];
         logA0[s] = g.logA0[r]; b0[s] = g.b0[r]; EaR0[s] = g.EaR0[r]; A0c[s] = g.A0[r];
-        if (g.type[r] == 3) {
+        if (g.type[r] == 3) {   // (type 4, PLOG, carries no falloff data)
             ta[s] = g.troe[4 * r + 0];
             tiT3[s] = 1.0 / g.troe[4 * r + 1];
             tiT1[s] = 1.0 / g.troe[4 * r + 2];
@@ -211,15 +260,17 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
         for (int i = 0; i < P; ++i) {
             int sp = g.prod_sp[r * P + i];
             if (sp < 0) break;
-            for (int q = 0; q < g.prod_nu[r * P + i]; ++q) {
-                // product factors only enter the reverse rate
-                if (!g.rev[r]) continue;
+            // product factors only enter the reverse rate
+            if (!g.rev[r]) continue;
+            const double nu = g.prod_nu[r * P + i];
+            if (nu != (double)(int)nu) { *err = "fractional product coefficient in a reversible reaction"; return HostMech(); }
+            for (int q = 0; q < (int)nu; ++q) {
                 if (npf >= 3) { *err = "more than 3 product molecules in a reversible reaction"; return HostMech(); }
                 pf[npf * ns + s] = sp; ++npf;
             }
-            d += g.prod_nu[r * P + i];
+            d += (int)nu;
         }
-        dnu[s] = d;
+        dnu[s] = g.rev[r] ? d : 0;   // enters Kc only
         lnPfac[s] = d * lnPR;
         tboff[s] = (int)tbsp.size();
         // a third-body list of all species but one with alpha = -1 is pyJac's
@@ -249,19 +300,25 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
         }
         tblen[s] = (int)tbsp.size() - tboff[s];
         // net stoichiometry rows
-        std::vector<std::pair<int, int>> net;
-        auto add = [&](int sp, int nu) {
+        std::vector<std::pair<int, double>> net;
+        auto add = [&](int sp, double nu) {
             for (auto& e : net) if (e.first == sp) { e.second += nu; return; }
             net.push_back({sp, nu});
         };
-        for (int i = 0; i < P; ++i) { int sp = g.reac_sp[r * P + i]; if (sp < 0) break; add(sp, -g.reac_nu[r * P + i]); }
+        for (int i = 0; i < P; ++i) { int sp = g.reac_sp[r * P + i]; if (sp < 0) break; add(sp, -(double)g.reac_nu[r * P + i]); }
         for (int i = 0; i < P; ++i) { int sp = g.prod_sp[r * P + i]; if (sp < 0) break; add(sp, g.prod_nu[r * P + i]); }
         int nrow = 0;
         for (auto& e : net) {
-            if (e.second == 0) continue;
-            if (nrow >= 6) { *err = "more than 6 species in one reaction"; return HostMech(); }
+            if (e.second == 0.0) continue;
+            if (nrow >= kJRow) { *err = "more than 8 species in one reaction"; return HostMech(); }
+            int sc = 0;
+            if (!scaled(e.second, &sc) || sc < -16 || sc > 15) {
+                *err = "net stoichiometric coefficient not encodable (multiple of 1/nu_den in [-16, 15] / nu_den)";
+                return HostMech();
+            }
             jrow[nrow * ns + s] = e.first;
             jnu[nrow * ns + s] = e.second;
+            jnu_scaled[nrow * ns + s] = sc;
             ++nrow;
         }
     }
@@ -275,8 +332,8 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
         spoff[k] = (int)spslot.size();
         for (int r = 0; r < nr; ++r) {
             int s = rxn_slot[r];
-            for (int e = 0; e < 6; ++e)
-                if (jrow[e * ns + s] == k) { spslot.push_back(s); spnu.push_back(jnu[e * ns + s]); }
+            for (int e = 0; e < kJRow; ++e)
+                if (jrow[e * ns + s] == k) { spslot.push_back(s); spnu.push_back(jnu_scaled[e * ns + s]); }
         }
     }
     spoff[n] = (int)spslot.size();
@@ -353,6 +410,16 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
     h.o_jrow = PUTV(jrow); h.o_jnu = PUTV(jnu); h.o_sp_off = PUTV(spoff);
     h.o_sp_slot = PUTV(spslot); h.o_sp_nu = PUTV(spnu);
     h.o_cat_sp = PUTV(catsp); h.o_gword = PUTV(gword); h.o_unit_off = PUTV(unitoff);
+    h.o_plog_lev0 = PUTV(plev0); h.o_plog_nlev = PUTV(pnlev);
+    h.o_plog_lnP = put(g.plog_lnP, g.nplog_lev * sizeof(double));
+    h.o_plog_toff = put(g.plog_term_off, (g.nplog_lev + 1) * sizeof(int));
+    h.o_plog_A = put(g.plog_A, g.nplog_term * sizeof(double));
+    h.o_plog_logA = put(g.plog_logA, g.nplog_term * sizeof(double));
+    h.o_plog_b = put(g.plog_b, g.nplog_term * sizeof(double));
+    h.o_plog_EaR = put(g.plog_EaR, g.nplog_term * sizeof(double));
+    std::vector<int> inert(n);
+    for (int k = 0; k < n; ++k) inert[k] = spoff[k + 1] == spoff[k];
+    h.o_inert = PUTV(inert);
 #undef PUTV
     h.blob.resize((h.blob.size() + 255) & ~size_t(255));
     return h;

@@ -62,9 +62,9 @@ ELEMENT_WEIGHTS = {
     "He": 4.002602, "HE": 4.002602, "E": 5.48579909e-4,
 }
 
-T_ELEMENTARY, T_THIRD_BODY, T_LINDEMANN, T_TROE = 0, 1, 2, 3
+T_ELEMENTARY, T_THIRD_BODY, T_LINDEMANN, T_TROE, T_PLOG = 0, 1, 2, 3, 4
 TYPE_NAMES = {T_ELEMENTARY: "elementary", T_THIRD_BODY: "three-body",
-              T_LINDEMANN: "lindemann", T_TROE: "troe"}
+              T_LINDEMANN: "lindemann", T_TROE: "troe", T_PLOG: "plog"}
 
 
 @dataclass
@@ -83,7 +83,7 @@ class Reaction:
     rtype: int
     reversible: bool
     reac: List[Tuple[int, int]]          # (species, stoich) in equation order
-    prod: List[Tuple[int, int]]
+    prod: List[Tuple[int, float]]        # fractional only in irreversible reactions
     A: float = 0.0                       # SI kmol units; high-P limit for falloff
     b: float = 0.0
     EaR: float = 0.0                     # activation temperature [K]
@@ -94,13 +94,17 @@ class Reaction:
     troe_has_T2: bool = False
     tb: List[Tuple[int, float]] = field(default_factory=list)  # (species, eff-1)
     catalyst: Optional[int] = None       # species made the sole third body
+    # pressure-dependent Arrhenius (PLOG): levels sorted by pressure, each
+    # (P [Pa], [(A [SI kmol units], b, Ea/R [K]), ...]) -- the rate at a level
+    # is the sum of its terms
+    plog: List[Tuple[float, List[Tuple[float, float, float]]]] = field(default_factory=list)
 
     @property
     def has_third_body(self) -> bool:
         return self.rtype != T_ELEMENTARY
 
-    def net_stoich(self, nsp: int) -> Dict[int, int]:
-        d: Dict[int, int] = {}
+    def net_stoich(self, nsp: int) -> Dict[int, float]:
+        d: Dict[int, float] = {}
         for s, nu in self.reac:
             d[s] = d.get(s, 0) - nu
         for s, nu in self.prod:
@@ -108,26 +112,28 @@ class Reaction:
         return {k: v for k, v in d.items() if v != 0}
 
 
-def _parse_side(side: str) -> List[Tuple[str, int]]:
-    out: List[Tuple[str, int]] = []
+def _nu(v: float):
+    """A stoichiometric coefficient: int when integral, else float."""
+    return int(v) if v == int(v) else float(v)
+
+
+def _parse_side(side: str) -> List[Tuple[str, float]]:
+    out: List[Tuple[str, float]] = []
     for tok in side.split(" + "):
         tok = tok.strip()
         if not tok:
             continue
         m = re.match(r"^(\d+(?:\.\d+)?)\s+(\S+)$", tok)
         if m:
-            nu = float(m.group(1))
-            if nu != int(nu):
-                raise NotImplementedError(f"non-integer stoichiometry: {tok}")
-            out.append((m.group(2), int(nu)))
+            out.append((m.group(2), _nu(float(m.group(1)))))
         else:
             out.append((tok, 1))
     return out
 
 
-def _merge(side: List[Tuple[str, int]]) -> List[Tuple[str, int]]:
+def _merge(side: List[Tuple[str, float]]) -> List[Tuple[str, float]]:
     order: List[str] = []
-    cnt: Dict[str, int] = {}
+    cnt: Dict[str, float] = {}
     for name, nu in side:
         if name not in cnt:
             order.append(name)
@@ -247,8 +253,10 @@ class Mechanism:
     @classmethod
     def from_ctml(cls, path: str, name: Optional[str] = None) -> "Mechanism":
         """Parse a Cantera CTML (XML) mechanism: NASA-7 species, Arrhenius,
-        three-body and Lindemann/Troe falloff reactions.  CTML stores A in SI
-        kmol units and names E's unit on each element."""
+        three-body, Lindemann/Troe falloff and pressure-dependent Arrhenius
+        (``type="plog"``) reactions, fractional product coefficients in
+        irreversible reactions.  CTML stores A in SI kmol units and names E's
+        (and P's) unit on each element."""
         import xml.etree.ElementTree as ET
         root = ET.parse(path).getroot()
         phase = root.find("phase")
@@ -277,14 +285,13 @@ class Mechanism:
         e_to_K = {"cal/mol": 4.184 / 8.3144621, "kcal/mol": 4184.0 / 8.3144621, "J/mol": 1.0 / 8.3144621,
                   "kJ/mol": 1000.0 / 8.3144621, "J/kmol": 1.0 / 8314.4621, "K": 1.0}
 
-        def side(text: str) -> List[Tuple[str, int]]:
+        p_to_Pa = {"atm": PA_ATM, "Pa": 1.0, "bar": 1.0e5}
+
+        def side(text: str) -> List[Tuple[str, float]]:
             out = []
             for tok in (text or "").split():
                 nm, nu = tok.rsplit(":", 1)
-                v = float(nu)
-                if v != int(v):
-                    raise NotImplementedError(f"non-integer stoichiometry: {tok}")
-                out.append((nm, int(v)))
+                out.append((nm, _nu(float(nu))))
             return _merge(out)
 
         reactions: List[Reaction] = []
@@ -298,13 +305,21 @@ class Mechanism:
                 raise NotImplementedError(f"reaction {i}: unsupported rate form")
             arr = {a.get("name", "rate"): a for a in rc.findall("Arrhenius")}
 
-            def rate(which: str, order: int, arr=arr):
-                a = arr["k0" if which == "low" else "rate"]
+            def arrhenius(a):
                 A = float(a.find("A").text)
                 if A < 0:
                     raise NotImplementedError("negative A")
                 Ee = a.find("E")
                 return A, float(a.find("b").text), float(Ee.text) * e_to_K[Ee.get("units", "cal/mol")]
+
+            def rate(which: str, order: int, arr=arr, rc=rc):
+                if which == "plog":
+                    levels: Dict[float, List[Tuple[float, float, float]]] = {}
+                    for a in rc.findall("Arrhenius"):
+                        pe = a.find("P")
+                        levels.setdefault(float(pe.text) * p_to_Pa[pe.get("units", "Pa")], []).append(arrhenius(a))
+                    return sorted(levels.items())
+                return arrhenius(arr["k0" if which == "low" else "rate"])
 
             troe = None
             fo = rc.find("falloff")
@@ -327,6 +342,8 @@ class Mechanism:
                 kind = "falloff"
             elif t == "elementary":
                 kind = "elementary"
+            elif t == "plog":
+                kind = "plog"
             else:
                 raise NotImplementedError(f"reaction {i}: type {t}")
             L, R = side(rxn.find("reactants").text), side(rxn.find("products").text)
@@ -342,8 +359,17 @@ class Mechanism:
         """One reaction with pyJac's conventions.  rate(key, order) gives
         (A [SI kmol units], b, Ea/R [K]) for the rate expression named key."""
         order = sum(nu for _, nu in L)
+        if any(nu != int(nu) for _, nu in L) or (rev and any(nu != int(nu) for _, nu in R)):
+            raise NotImplementedError(f"reaction {i}: fractional stoichiometry outside the products "
+                                      f"of an irreversible reaction")
         rx = Reaction(index=i, equation=eq, rtype=T_ELEMENTARY, reversible=rev, reac=[], prod=[])
-        if kind == "elementary":
+        if kind == "plog":
+            # k(T, P): ln k interpolated linearly in ln P between the bracketing
+            # levels, clamped to the end levels (Cantera's PlogRate)
+            rx.rtype = T_PLOG
+            rx.plog = [(p, list(terms)) for p, terms in rate("plog", order)]
+            rx.A, rx.b, rx.EaR = rx.plog[0][1][0]
+        elif kind == "elementary":
             rx.A, rx.b, rx.EaR = rate(k_elem, order)
             # pyJac: in a termolecular step (three molecules on either
             # side) a species found on both sides becomes the sole third
@@ -352,7 +378,8 @@ class Mechanism:
             lnames = {n for n, _ in L}
             common = [n for n, _ in R if n in lnames]
             termolecular = max(sum(nu for _, nu in L), sum(nu for _, nu in R)) >= 3
-            if common and termolecular:
+            integral = all(nu == int(nu) for _, nu in R)   # lumped steps with fractional
+            if common and termolecular and integral:         # products stay elementary
                 if len(common) != 1:
                     raise NotImplementedError(f"reaction {i}: several catalysts")
                 c = common[0]
@@ -450,9 +477,41 @@ class Mechanism:
             tb_sp, tb_al = [0], [0.0]
         logA = [math.log(r.A) if r.A > 0 else 0.0 for r in self.reactions]
         logA0 = [math.log(r.A0) if r.A0 > 0 else 0.0 for r in self.reactions]
+        # denominator that makes every product coefficient integral (kernels
+        # encode nu * NU_DEN in small integer fields)
+        nu_den = next((d for d in (1, 2, 4) if all(abs(v * d - round(v * d)) < 1e-12
+                                                   for r in self.reactions for _, v in r.prod)), None)
+        if nu_den is None:
+            raise NotImplementedError("product coefficients need a denominator above 4")
+        # PLOG tables: reaction r's levels are plog_off[r] .. plog_off[r+1]-1;
+        # level l's Arrhenius terms are plog_term_off[l] .. plog_term_off[l+1]-1
+        plog_off, plog_lnP, plog_toff = [0], [], [0]
+        plog_A, plog_b, plog_EaR = [], [], []
+        for r in self.reactions:
+            for P_, terms in r.plog:
+                plog_lnP.append(math.log(P_))
+                for A_, b_, E_ in terms:
+                    plog_A.append(A_)
+                    plog_b.append(b_)
+                    plog_EaR.append(E_)
+                plog_toff.append(len(plog_A))
+            plog_off.append(len(plog_lnP))
+        nlev, nterm = max(len(plog_lnP), 1), max(len(plog_A), 1)
+        if not plog_lnP:
+            plog_lnP, plog_A, plog_b, plog_EaR = [0.0], [0.0], [0.0], [0.0]
+            plog_toff = [0, 0]
+        plog_logA = [math.log(a) if a > 0 else 0.0 for a in plog_A]
+        # units of the kernels' balanced species gather: each species' (reaction,
+        # net coefficient) entries cut into runs of at most 24 (kGatherUnit in
+        # csrc/mech_dev.h); sizes the per-warp shared scratch exactly
+        entries = [0] * n
+        for r in self.reactions:
+            for k in r.net_stoich(n):
+                entries[k] += 1
+        n_units = sum(-(-e // 24) for e in entries)
         lines = []
         w = lines.append
-        w(f"/* Generated by hpc_ode_b200/mechanism.py from {self.name}.yaml -- do not edit. */")
+        w(f"/* Generated by hpc_ode_b200/mechanism.py from {self.name} -- do not edit. */")
         w(f"#ifndef {pfx}_H")
         w(f"#define {pfx}_H")
         w(f"/* {self.counts()} */")
@@ -460,6 +519,11 @@ class Mechanism:
         w(f"#define {pfx}_NRXN {nr}")
         w(f"#define {pfx}_MAXP {P}")
         w(f"#define {pfx}_NTB {len(tb_sp)}")
+        w(f"#define {pfx}_NU_DEN {nu_den}")
+        w(f"#define {pfx}_NUNITS {n_units}")
+        w(f"#define {pfx}_NPLOG {sum(r.rtype == T_PLOG for r in self.reactions)}")
+        w(f"#define {pfx}_NPLOGLEV {nlev}")
+        w(f"#define {pfx}_NPLOGTERM {nterm}")
         w(f"static const char* const {tag}_species_names[{n}] = {{{', '.join(chr(34)+s.name+chr(34) for s in self.species)}}};")
         w(f"static const double {tag}_mw[{n}] = {{{fa(s.mw for s in self.species)}}};")
         w(f"static const double {tag}_tmid[{n}] = {{{fa(s.tmid for s in self.species)}}};")
@@ -480,10 +544,17 @@ class Mechanism:
         w(f"static const int {tag}_rxn_reac_sp[{nr * P}] = {{{ia(reac_sp)}}};")
         w(f"static const int {tag}_rxn_reac_nu[{nr * P}] = {{{ia(reac_nu)}}};")
         w(f"static const int {tag}_rxn_prod_sp[{nr * P}] = {{{ia(prod_sp)}}};")
-        w(f"static const int {tag}_rxn_prod_nu[{nr * P}] = {{{ia(prod_nu)}}};")
+        w(f"static const double {tag}_rxn_prod_nu[{nr * P}] = {{{fa(prod_nu)}}};")
         w(f"static const int {tag}_rxn_tb_off[{nr + 1}] = {{{ia(tb_off)}}};")
         w(f"static const int {tag}_tb_sp[{len(tb_sp)}] = {{{ia(tb_sp)}}};")
         w(f"static const double {tag}_tb_alpha[{len(tb_al)}] = {{{fa(tb_al)}}};")
+        w(f"static const int {tag}_plog_off[{nr + 1}] = {{{ia(plog_off)}}};")
+        w(f"static const double {tag}_plog_lnP[{nlev}] = {{{fa(plog_lnP)}}};")
+        w(f"static const int {tag}_plog_term_off[{nlev + 1}] = {{{ia(plog_toff)}}};")
+        w(f"static const double {tag}_plog_A[{nterm}] = {{{fa(plog_A)}}};")
+        w(f"static const double {tag}_plog_logA[{nterm}] = {{{fa(plog_logA)}}};")
+        w(f"static const double {tag}_plog_b[{nterm}] = {{{fa(plog_b)}}};")
+        w(f"static const double {tag}_plog_EaR[{nterm}] = {{{fa(plog_EaR)}}};")
         w(f"#endif /* {pfx}_H */")
         os.makedirs(os.path.dirname(path), exist_ok=True)
         with open(path, "w") as f:
@@ -512,7 +583,8 @@ MECH_DIR_ENV = "HPC_ODE_MECH_DIR"
 
 def load(name: str, mech_dir: Optional[str] = None) -> Mechanism:
     """Parse ``<mech_dir>/<name>.yaml``, or ``<name>.xml`` (CTML) when there is
-    no YAML file (``gri30``, ``h2o2``, ``nDodecane_Reitz``, ``h2_li_2004``)."""
+    no YAML file (``gri30``, ``h2o2``, ``nDodecane_Reitz``, ``h2_li_2004``,
+    ``ESTiMatE-Mech_04042022``)."""
     base = os.path.splitext(name)[0] if name.endswith((".yaml", ".xml")) else name
     mech_dir = mech_dir or os.environ.get(MECH_DIR_ENV)
     if not mech_dir:
@@ -526,7 +598,7 @@ def load(name: str, mech_dir: Optional[str] = None) -> Mechanism:
 def generate_all(mech_dir: Optional[str] = None, out_dir: Optional[str] = None) -> List[str]:
     out_dir = out_dir or os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "mech")
     paths = []
-    for nm in ("gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004"):
+    for nm in ("gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004", "ESTiMatE-Mech_04042022"):
         m = load(nm, mech_dir)
         p = os.path.join(out_dir, f"{nm}_mech.h")
         m.emit_header(p)

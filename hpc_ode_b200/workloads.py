@@ -17,6 +17,10 @@ Workloads (all rtol 1e-6, atol 1e-10):
                T0 = linspace(1000,2100,100) x phi = linspace(0.5,3.5,100), P = 101325.15 Pa, dt 1e-3 s
   nc12_8k      nDodecane_Reitz (100 species, 553 reactions), 8,192 cells, P ~ U[10,60] atm,
                T0 ~ U[800,1600] K, n-dodecane/air phi ~ U[0.5,2.0], dt 1e-4 s
+  kero_2k      ESTiMatE-Mech_04042022 (214 species, 1,558 reactions), 2,048 cells, P ~ U[5,40] atm,
+               T0 ~ U[900,1800] K, kerosene surrogate (60 % n-C12H26, 20 % i-C8H18, 20 % toluene
+               by mole)/air phi ~ U[0.5,2.0], dt 1e-4 s.  The reference's ESTiMatE dataset
+               (ref_data/res_est.csv) is not distributed, so this stands in for it.
 """
 from __future__ import annotations
 
@@ -29,6 +33,7 @@ import numpy as np
 
 MECH_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "mech")
 ATM = 101325.0
+ESTIMATE = "ESTiMatE-Mech_04042022"
 
 
 def mech_info(mech: str) -> Dict:
@@ -80,6 +85,14 @@ def premixed_Y(mech: str, fuel: str, phi: np.ndarray) -> np.ndarray:
         X[idx["CH4"]] = phi
         X[idx["O2"]] = 2.0
         X[idx["N2"]] = 7.52
+    elif fuel == "kerosene":
+        # three-component kerosene surrogate (mole fractions of the fuel):
+        # 60 % n-dodecane, 20 % iso-octane, 20 % toluene; O2 demand per mole
+        # of fuel 0.6 * 18.5 + 0.2 * 12.5 + 0.2 * 9 = 15.4
+        for nm, x in (("N-C12H26", 0.6), ("I-C8H18", 0.2), ("C7H8", 0.2)):
+            X[idx[nm]] = x * phi
+        X[idx["O2"]] = 15.4
+        X[idx["N2"]] = 15.4 * 3.76
     elif fuel == "C12H26":
         # C12H26 + 18.5 (O2 + 3.76 N2)
         X[idx["C12H26"]] = phi
@@ -126,6 +139,12 @@ def make(name: str, ncells: Optional[int] = None, seed: Optional[int] = None) ->
         P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
         Y = premixed_Y("nDodecane_Reitz", "C12H26", phi)
         mech = "nDodecane_Reitz"
+    elif kind == "kerosene":
+        T = rng.uniform(cfg["T"][0], cfg["T"][1], n)
+        phi = rng.uniform(cfg["phi"][0], cfg["phi"][1], n)
+        P = rng.uniform(cfg["P_atm"][0], cfg["P_atm"][1], n) * ATM
+        Y = premixed_Y(ESTIMATE, "kerosene", phi)
+        mech = ESTIMATE
     elif kind == "gri_bimodal":
         cold = rng.uniform(0.0, 1.0, n) < 0.7
         T = np.where(cold, rng.uniform(300.0, 900.0, n), rng.uniform(1100.0, 2200.0, n))
@@ -150,6 +169,10 @@ WORKLOADS = {
     # larger mechanism (100 species, 553 reactions): diesel-like n-dodecane/air
     "nc12_8k": dict(kind="ndodecane", ncells=8192, dt=1e-4, seed=6, T=(800.0, 1600.0),
                     phi=(0.5, 2.0), P_atm=(10.0, 60.0)),
+    # largest mechanism (214 species, 1,558 reactions with PLOG and lumped
+    # steps): kerosene-surrogate/air at gas-turbine pressures
+    "kero_2k": dict(kind="kerosene", ncells=2048, dt=1e-4, seed=8, T=(900.0, 1800.0),
+                    phi=(0.5, 2.0), P_atm=(5.0, 40.0)),
 }
 RTOL, ATOL = 1e-6, 1e-10
 

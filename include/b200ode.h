@@ -98,7 +98,10 @@ typedef struct {
 void b200ode_default_options(b200ode_options* opts);
 
 /* Create a handle for a mechanism compiled into the library: "gri30", "h2o2",
- * "nDodecane_Reitz" (".yaml" suffix optional) or "h2_li_2004" (".xml" optional).
+ * "nDodecane_Reitz" (".yaml" suffix optional), "h2_li_2004" or
+ * "ESTiMatE-Mech_04042022" (".xml" optional).  ESTiMatE (214 species) runs in
+ * B200ODE_MIXED only: its FP64 Newton matrix exceeds an SM's shared memory
+ * (B200ODE_ERR_INVALID).
  * Replaces the per-batch set-up of CVodeIntegratorGPU::integrateBatch
  * (CVodeIntegratorGPU.cpp:44-100) and CVodeIntegrator::init's NSP check
  * (CVodeIntegrator.cpp:34-50).  opts may be NULL (defaults). */

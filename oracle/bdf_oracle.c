@@ -657,10 +657,12 @@ long oracle_bdf_batch_mech(int mech, long ncells, const double* pres, double pre
                            oracle_bdf_stats* stats, int nthreads) {
     oracle_rhs_fn f = mech == ORACLE_MECH_GRI30 ? oracle_gri30_dydt
                       : mech == ORACLE_MECH_H2O2 ? oracle_h2o2_dydt
-                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_dydt : oracle_ndodecane_dydt;
+                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_dydt
+                      : mech == ORACLE_MECH_ESTIMATE ? oracle_estimate_dydt : oracle_ndodecane_dydt;
     oracle_jac_fn J = mech == ORACLE_MECH_GRI30 ? oracle_gri30_jacob
                       : mech == ORACLE_MECH_H2O2 ? oracle_h2o2_jacob
-                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_jacob : oracle_ndodecane_jacob;
+                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_jacob
+                      : mech == ORACLE_MECH_ESTIMATE ? oracle_estimate_jacob : oracle_ndodecane_jacob;
     return oracle_bdf_batch(f, J, oracle_mech_nsp(mech), ncells, pres, pres_scalar, y, t0, tout,
                             opts, stats, nthreads);
 }

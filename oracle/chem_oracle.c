@@ -9,6 +9,12 @@
  *   eval_cp / eval_h   src/Mechanism/CPU/chem_utils.c:194,1160
  *   dydt               src/Mechanism/CPU/dydt.c:7-133
  *   eval_jacob         src/Mechanism/CPU/jacob.c:3-372 (exact derivative of dydt)
+ * and, for mechanisms the reference integrates only through Cantera
+ * (src/Integrators/CanteraIntegrator.cpp), the rate forms pyJac's tables do
+ * not cover: pressure-dependent Arrhenius (PLOG) reactions and fractional
+ * product coefficients of irreversible reactions, with Cantera's published
+ * PLOG definition (ln k linear in ln P between the bracketing levels, clamped
+ * to the end levels; a level's k is the sum of its Arrhenius terms).
  * The Jacobian is derived here from the RHS (chain rule through the
  * concentrations and the closure species), not from pyJac's expression
  * layout; it agrees with pyJac's to round-off.
@@ -23,18 +29,24 @@
 #include "../hpc_ode_b200/csrc/mech/h2o2_mech.h"
 #include "../hpc_ode_b200/csrc/mech/nDodecane_Reitz_mech.h"
 #include "../hpc_ode_b200/csrc/mech/h2_li_2004_mech.h"
+#include "../hpc_ode_b200/csrc/mech/ESTiMatE-Mech_04042022_mech.h"
 
 #define RU 8314.4621
 #define PATM 101325.0
-#define MAXNSP 128
+#define MAXNSP 256
+#define MAXP_ORACLE 8   /* participants per side (the generated MAXP is at most this) */
 
 typedef struct {
     int nsp, nrxn, maxp;
     const double *mw, *tmid, *lo, *hi;
     const int *type, *rev;
     const double *A, *logA, *b, *EaR, *A0, *logA0, *b0, *EaR0, *troe;
-    const int *troeT2, *reac_sp, *reac_nu, *prod_sp, *prod_nu, *tb_off, *tb_sp;
+    const int *troeT2, *reac_sp, *reac_nu, *prod_sp;
+    const double *prod_nu;   /* fractional only in irreversible reactions */
+    const int *tb_off, *tb_sp;
     const double *tb_alpha;
+    const int *plog_off, *plog_term_off;
+    const double *plog_lnP, *plog_A, *plog_logA, *plog_b, *plog_EaR;
 } mech_t;
 
 #define MECH_INIT(tag, PFX) { PFX##_NSP, PFX##_NRXN, PFX##_MAXP, \
@@ -42,11 +54,18 @@ typedef struct {
     tag##_rxn_A, tag##_rxn_logA, tag##_rxn_b, tag##_rxn_EaR, tag##_rxn_A0, tag##_rxn_logA0, \
     tag##_rxn_b0, tag##_rxn_EaR0, tag##_rxn_troe, tag##_rxn_troe_T2, tag##_rxn_reac_sp, \
     tag##_rxn_reac_nu, tag##_rxn_prod_sp, tag##_rxn_prod_nu, tag##_rxn_tb_off, tag##_tb_sp, \
-    tag##_tb_alpha }
+    tag##_tb_alpha, tag##_plog_off, tag##_plog_term_off, tag##_plog_lnP, tag##_plog_A, \
+    tag##_plog_logA, tag##_plog_b, tag##_plog_EaR }
 
-static const mech_t MECHS[4] = { MECH_INIT(gri30, MECH_GRI30), MECH_INIT(h2o2, MECH_H2O2),
-                                 MECH_INIT(ndodecane_reitz, MECH_NDODECANE_REITZ),
-                                 MECH_INIT(h2_li_2004, MECH_H2_LI_2004) };
+#define NMECH 5
+#if MECH_GRI30_MAXP > MAXP_ORACLE || MECH_ESTIMATE_MECH_04042022_MAXP > MAXP_ORACLE || \
+    MECH_NDODECANE_REITZ_MAXP > MAXP_ORACLE
+#error "participant lists longer than the oracle's scratch"
+#endif
+static const mech_t MECHS[NMECH] = { MECH_INIT(gri30, MECH_GRI30), MECH_INIT(h2o2, MECH_H2O2),
+                                     MECH_INIT(ndodecane_reitz, MECH_NDODECANE_REITZ),
+                                     MECH_INIT(h2_li_2004, MECH_H2_LI_2004),
+                                     MECH_INIT(estimate_mech_04042022, MECH_ESTIMATE_MECH_04042022) };
 
 int oracle_mech_id(const char* name) {
     if (!name) return -1;
@@ -54,11 +73,12 @@ int oracle_mech_id(const char* name) {
     if (!strncmp(name, "h2o2", 4)) return ORACLE_MECH_H2O2;
     if (!strncmp(name, "nDodecane_Reitz", 15)) return ORACLE_MECH_NDODECANE;
     if (!strncmp(name, "h2_li_2004", 10)) return ORACLE_MECH_H2LI;
+    if (!strncmp(name, "ESTiMatE-Mech_04042022", 22)) return ORACLE_MECH_ESTIMATE;
     return -1;
 }
 
 int oracle_mech_nsp(int mech) {
-    if (mech < 0 || mech > 3) return -1;
+    if (mech < 0 || mech >= NMECH) return -1;
     return MECHS[mech].nsp;
 }
 
@@ -98,10 +118,44 @@ static double arrh(double A, double logA, double b, double EaR, double logT, dou
     return exp(logA + b * logT - EaR / T);
 }
 
+/* k of PLOG level l (sum of its Arrhenius terms) and d ln k / dT. */
+static double plog_level(const mech_t* M, int l, double T, double logT, double* dlnk_dT) {
+    double k = 0.0, dk = 0.0;
+    for (int t = M->plog_term_off[l]; t < M->plog_term_off[l + 1]; ++t) {
+        double kt = arrh(M->plog_A[t], M->plog_logA[t], M->plog_b[t], M->plog_EaR[t], logT, T);
+        k += kt;
+        dk += kt * (M->plog_b[t] + M->plog_EaR[t] / T) / T;
+    }
+    *dlnk_dT = dk / k;
+    return k;
+}
+
+/* PLOG rate of reaction r at (T, P): ln k linear in ln P between the levels
+ * that bracket P, the end level's k outside their range. */
+static double plog_rate(const mech_t* M, int r, double T, double logT, double lnP, double* dlnk_dT) {
+    const int l0 = M->plog_off[r], l1 = M->plog_off[r + 1] - 1;
+    int lo = l0, hi = l0;
+    double w = 0.0;
+    if (lnP >= M->plog_lnP[l1]) {
+        lo = hi = l1;
+    } else if (lnP > M->plog_lnP[l0]) {
+        while (M->plog_lnP[lo + 1] < lnP) ++lo;
+        hi = lo + 1;
+        w = (lnP - M->plog_lnP[lo]) / (M->plog_lnP[hi] - M->plog_lnP[lo]);
+    }
+    double d0, d1;
+    const double k0 = plog_level(M, lo, T, logT, &d0);
+    const double k1 = plog_level(M, hi, T, logT, &d1);
+    *dlnk_dT = (1.0 - w) * d0 + w * d1;
+    return exp((1.0 - w) * log(k0) + w * log(k1));
+}
+
 static void eval_reaction(const mech_t* M, int r, double T, double logT, double m,
                           const double* C, const double* mgRT, int want_deriv, rxn_eval_t* o) {
     const int P = M->maxp;
-    double kf = arrh(M->A[r], M->logA[r], M->b[r], M->EaR[r], logT, T);
+    double dlnkf_dT = (M->b[r] + M->EaR[r] / T) / T;
+    double kf = M->type[r] == 4 ? plog_rate(M, r, T, logT, log(m * RU * T), &dlnkf_dT)
+                                : arrh(M->A[r], M->logA[r], M->b[r], M->EaR[r], logT, T);
     double Rf = 1.0, Rr = 1.0;
     int ordf = 0, ordr = 0, dnu = 0;
     double sum_g = 0.0;
@@ -112,16 +166,16 @@ static void eval_reaction(const mech_t* M, int r, double T, double logT, double 
         for (int q = 0; q < nu; ++q) Rf *= C[s];
         ordf += nu; dnu -= nu; sum_g -= nu * mgRT[s];
     }
-    for (int i = 0; i < P; ++i) {
+    for (int i = 0; M->rev[r] && i < P; ++i) {   /* products enter the reverse rate only */
         int s = M->prod_sp[r * P + i];
         if (s < 0) break;
-        int nu = M->prod_nu[r * P + i];
+        int nu = (int)M->prod_nu[r * P + i];
         for (int q = 0; q < nu; ++q) Rr *= C[s];
         ordr += nu; dnu += nu; sum_g += nu * mgRT[s];
     }
     o->ordf = ordf; o->ordr = ordr;
     o->kf = kf;
-    o->dlnkf_dT = (M->b[r] + M->EaR[r] / T) / T;
+    o->dlnkf_dT = dlnkf_dT;
     if (M->rev[r]) {
         /* Kc = exp(sum nu (s/R - h/RT)) * (Patm / (R T))^dnu */
         double Kc = exp(sum_g - dnu * logT) * pow(PATM / RU, (double)dnu);
@@ -135,7 +189,7 @@ static void eval_reaction(const mech_t* M, int r, double T, double logT, double 
     o->Rr = o->kr * Rr;
     o->phi = 1.0; o->thd = 0.0; o->dphi_dthd = 0.0; o->dphi_dT = 0.0;
     int type = M->type[r];
-    if (type == 0) return;
+    if (type == 0 || type == 4) return;
     double thd = m;
     for (int t = M->tb_off[r]; t < M->tb_off[r + 1]; ++t) thd += M->tb_alpha[t] * C[M->tb_sp[t]];
     o->thd = thd;
@@ -178,6 +232,20 @@ static void eval_reaction(const mech_t* M, int r, double T, double logT, double 
         o->dphi_dthd = dphi_dPr * (k0 / kf);
         double dlnPr_dT = (M->b0[r] + M->EaR0[r] / T) / T - (M->b[r] + M->EaR[r] / T) / T;
         o->dphi_dT = dphi_dPr * Pr * dlnPr_dT + blend * F * log(10.0) * dlog10F_dT;
+    }
+}
+
+/* Forward rate coefficient of every reaction at (T, P) (for falloff
+ * reactions the high-pressure limit); kf[nrxn]. */
+void oracle_kf(int mech, double pres, double T, double* kf) {
+    const mech_t* M = &MECHS[mech];
+    static const double zero[MAXNSP];
+    double C[MAXNSP];
+    for (int k = 0; k < M->nsp; ++k) C[k] = 1.0;
+    for (int r = 0; r < M->nrxn; ++r) {
+        rxn_eval_t e;
+        eval_reaction(M, r, T, log(T), pres / (RU * T), C, zero, 0, &e);
+        kf[r] = e.kf;
     }
 }
 
@@ -273,6 +341,13 @@ void oracle_dydt_scale(int mech, double pres, const double* y, double* scale) {
 }
 
 /* -------------------------------------------------------------- Jacobian */
+
+/* Stoichiometric coefficient of entry e of the reactant (side 0) or product
+ * (side 1) list. */
+static double stoich(const mech_t* M, int side, int e) {
+    return side ? M->prod_nu[e] : (double)M->reac_nu[e];
+}
+
 void oracle_jacob(int mech, double pres, const double* y, double* jac) {
     const mech_t* M = &MECHS[mech];
     const int n = M->nsp, P = M->maxp;
@@ -292,7 +367,7 @@ void oracle_jacob(int mech, double pres, const double* y, double* jac) {
         double q = R * e.phi;
         /* d ln kr / dT = d ln kf / dT - d ln Kc / dT,
            d ln Kc / dT = (sum nu h/RT - dnu) / T */
-        double dH = 0.0; int dnu = 0;
+        double dH = 0.0, dnu = 0.0;
         for (int i = 0; i < P; ++i) { int sp = M->reac_sp[r * P + i]; if (sp < 0) break; dH -= M->reac_nu[r * P + i] * s.hRT[sp]; dnu -= M->reac_nu[r * P + i]; }
         for (int i = 0; i < P; ++i) { int sp = M->prod_sp[r * P + i]; if (sp < 0) break; dH += M->prod_nu[r * P + i] * s.hRT[sp]; dnu += M->prod_nu[r * P + i]; }
         double dlnkr = M->rev[r] ? e.dlnkf_dT - (dH - dnu) / T : 0.0;
@@ -302,20 +377,19 @@ void oracle_jacob(int mech, double pres, const double* y, double* jac) {
         double dq_dT = e.phi * dR_dT + R * e.dphi_dT - (Sr + thd_term * e.thd) / T;
         double s_r = Sr + thd_term * (e.thd - s.m);         /* sum_i dq/dC_i C_i */
         /* dq/dC_j for mass-action participants */
-        double dqdC[2 * 4];
-        int jsp[2 * 4], nj = 0;
-        for (int side = 0; side < 2; ++side) {
+        double dqdC[2 * MAXP_ORACLE];
+        int jsp[2 * MAXP_ORACLE], nj = 0;
+        for (int side = 0; side < 1 + M->rev[r]; ++side) {   /* products: reverse rate only */
             const int* sp_t = side ? M->prod_sp : M->reac_sp;
-            const int* nu_t = side ? M->prod_nu : M->reac_nu;
             double kcoef = side ? -e.kr : e.kf;
             for (int i = 0; i < P; ++i) {
                 int sp = sp_t[r * P + i];
                 if (sp < 0) break;
-                double d = kcoef * nu_t[r * P + i];
+                double d = kcoef * stoich(M, side, r * P + i);
                 for (int i2 = 0; i2 < P; ++i2) {
                     int sp2 = sp_t[r * P + i2];
                     if (sp2 < 0) break;
-                    int nu2 = nu_t[r * P + i2] - (i2 == i ? 1 : 0);
+                    int nu2 = (int)stoich(M, side, r * P + i2) - (i2 == i ? 1 : 0);
                     for (int qq = 0; qq < nu2; ++qq) d *= s.C[sp2];
                 }
                 jsp[nj] = sp; dqdC[nj] = d * e.phi; ++nj;
@@ -324,12 +398,11 @@ void oracle_jacob(int mech, double pres, const double* y, double* jac) {
         /* scatter into rows of species with nonzero net stoichiometry */
         for (int side = 0; side < 2; ++side) {
             const int* sp_t = side ? M->prod_sp : M->reac_sp;
-            const int* nu_t = side ? M->prod_nu : M->reac_nu;
             double sg = side ? 1.0 : -1.0;
             for (int i = 0; i < P; ++i) {
                 int k = sp_t[r * P + i];
                 if (k < 0) break;
-                double nu = sg * nu_t[r * P + i];
+                double nu = sg * stoich(M, side, r * P + i);
                 s.omega[k] += nu * q;
                 domega_dT[k] += nu * dq_dT;
                 sk[k] += nu * s_r;
@@ -385,3 +458,5 @@ void oracle_ndodecane_dydt(double t, double pres, const double* y, double* dy) {
 void oracle_ndodecane_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_NDODECANE, pres, y, jac); }
 void oracle_h2li_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_H2LI, pres, y, dy); }
 void oracle_h2li_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_H2LI, pres, y, jac); }
+void oracle_estimate_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_ESTIMATE, pres, y, dy); }
+void oracle_estimate_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_ESTIMATE, pres, y, jac); }

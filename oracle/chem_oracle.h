@@ -22,7 +22,8 @@ extern "C" {
 #endif
 
 /* Mechanism ids. */
-enum { ORACLE_MECH_GRI30 = 0, ORACLE_MECH_H2O2 = 1, ORACLE_MECH_NDODECANE = 2, ORACLE_MECH_H2LI = 3 };
+enum { ORACLE_MECH_GRI30 = 0, ORACLE_MECH_H2O2 = 1, ORACLE_MECH_NDODECANE = 2, ORACLE_MECH_H2LI = 3,
+       ORACLE_MECH_ESTIMATE = 4 };
 
 int oracle_mech_id(const char* name);      /* "gri30"/"gri30.yaml"/"h2o2"... ; -1 if unknown */
 int oracle_mech_nsp(int mech);             /* number of species == state length */
@@ -36,10 +37,16 @@ void oracle_ndodecane_dydt(double t, double pres, const double* y, double* dy);
 void oracle_ndodecane_jacob(double t, double pres, const double* y, double* jac);
 void oracle_h2li_dydt(double t, double pres, const double* y, double* dy);
 void oracle_h2li_jacob(double t, double pres, const double* y, double* jac);
+void oracle_estimate_dydt(double t, double pres, const double* y, double* dy);
+void oracle_estimate_jacob(double t, double pres, const double* y, double* jac);
 
 /* Generic forms. */
 void oracle_dydt(int mech, double pres, const double* y, double* dy);
 void oracle_jacob(int mech, double pres, const double* y, double* jac);
+
+/* Forward rate coefficient of every reaction at (T, P), kf[nrxn] (falloff:
+ * the high-pressure limit; PLOG: interpolated in ln P). */
+void oracle_kf(int mech, double pres, double T, double* kf);
 
 /* Magnitude companion of dydt: |dy|-scale built from |forward| + |reverse|
  * contributions, used by tests to form cancellation-aware tolerances. */

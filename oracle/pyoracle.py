@@ -40,7 +40,7 @@ STATS_DTYPE = np.dtype([("status", "i4"), ("nst", "i4"), ("nfe", "i4"), ("nje", 
                         ("qlast", "i4"), ("pad", "i4"), ("hlast", "f8")])
 assert STATS_DTYPE.itemsize == C.sizeof(BdfStats)
 
-MECH_IDS = {"gri30": 0, "h2o2": 1, "nDodecane_Reitz": 2, "h2_li_2004": 3}
+MECH_IDS = {"gri30": 0, "h2o2": 1, "nDodecane_Reitz": 2, "h2_li_2004": 3, "ESTiMatE-Mech_04042022": 4}
 
 
 def build(force: bool = False) -> None:
@@ -64,6 +64,8 @@ class Oracle:
         for nm in ("oracle_dydt", "oracle_jacob", "oracle_dydt_scale"):
             getattr(L, nm).argtypes = [C.c_int, C.c_double, _dptr, _dptr]
             getattr(L, nm).restype = None
+        L.oracle_kf.argtypes = [C.c_int, C.c_double, C.c_double, _dptr]
+        L.oracle_kf.restype = None
         L.oracle_bdf_batch_mech.restype = C.c_long
         L.oracle_bdf_batch_mech.argtypes = [C.c_int, C.c_long, _dptr, C.c_double, _dptr, C.c_double,
                                             C.c_double, C.POINTER(BdfOpts), C.c_void_p, C.c_int]
@@ -87,6 +89,12 @@ class Oracle:
         y = np.ascontiguousarray(y, dtype=np.float64)
         out = np.zeros_like(y)
         self.lib.oracle_dydt_scale(MECH_IDS[mech], float(pres), _p(y), _p(out))
+        return out
+
+    def kf(self, mech: str, pres: float, T: float, nrxn: int) -> np.ndarray:
+        """Forward rate coefficient of every reaction at (T, P)."""
+        out = np.zeros(nrxn)
+        self.lib.oracle_kf(MECH_IDS[mech], float(pres), float(T), _p(out))
         return out
 
     def jacob(self, mech: str, pres: float, y: np.ndarray) -> np.ndarray:

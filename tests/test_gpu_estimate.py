@@ -1,0 +1,112 @@
+"""The largest mechanism (ESTiMatE kerosene: 214 species, 1,558 reactions with
+22 pressure-dependent Arrhenius (PLOG) reactions and lumped irreversible steps
+with fractional product coefficients; 7 elements per lane in the warp layout,
+one warp per SM) through the C ABI against the oracle.
+
+The reference integrates this mechanism only through Cantera
+(src/Integrators/CanteraIntegrator.cpp) and ships no kernels or results for it
+(ref_data/res_est.csv is not distributed), so the oracle is the table-driven C
+restatement: its tables come from the same generator that the GRI golden
+vectors pin, its PLOG rates are checked against a numpy restatement and its
+Jacobian against central differences of its RHS on the CPU
+(tests/test_oracle.py).  The FP64 Newton matrix does not fit in an SM's shared
+memory, so this mechanism runs in mixed precision only; the RHS is FP64 in
+either precision.
+"""
+import numpy as np
+import pytest
+
+from hpc_ode_b200 import native, workloads as W
+from conftest import y_ok
+
+GATE_T = 1e-5
+
+pytestmark = pytest.mark.gpu
+
+MECH = W.ESTIMATE
+
+
+def _cells(n, seed=3):
+    return W.make("kero_2k", n, seed=seed)
+
+
+def test_fp64_is_refused_with_a_reason():
+    with pytest.raises(native.B200Error) as e:
+        native.Solver(MECH, precision=native.B200ODE_FP64)
+    assert e.value.code == 1 and "MIXED only" in str(e.value)
+
+
+def test_rhs_matches_oracle(oracle):
+    """PLOG cells span the tabulated pressures (5-40 atm against levels at
+    0.01, 0.1, 1, 10, 100 atm), so both the interpolation and the clamped ends
+    of some tables are exercised."""
+    b = _cells(24)
+    b.P[:4] = np.array([0.003, 0.05, 150.0, 1.0]) * W.ATM
+    s = native.Solver(MECH)
+    dT, dY = s.eval_rhs(b.T, b.Y, b.P)
+    s.close()
+    got = np.concatenate([dT[:, None], dY.T], axis=1)
+    rows = b.state_rows()
+    for i in range(b.ncells):
+        ref = oracle.dydt(MECH, b.P[i], rows[i])
+        scale = oracle.dydt_scale(MECH, b.P[i], rows[i])
+        err = np.abs(got[i] - ref) / (np.abs(ref) + scale + np.abs(ref[1:]).max())
+        assert err.max() <= 1e-12, (i, err.max())
+
+
+def test_jacobian_matches_oracle(oracle):
+    b = _cells(6, seed=4)
+    b.P[0] = 0.05 * W.ATM
+    s = native.Solver(MECH)
+    J = s.eval_jacobian(b.T, b.Y, b.P)
+    s.close()
+    rows = b.state_rows()
+    for i in range(b.ncells):
+        Jo = oracle.jacob(MECH, b.P[i], rows[i])
+        mask = np.abs(Jo) > 1e-8 * np.abs(Jo).max()
+        rel = np.abs(J[i] - Jo)[mask] / np.abs(Jo)[mask]
+        assert rel.max() <= 1e-4, (i, rel.max())
+
+
+def test_integration_matches_oracle(oracle):
+    """Against the CPU integrator at the same tolerances, judged as for
+    n-dodecane (tests/test_gpu_ndodecane.py): most cells ignite within the
+    step, so the per-cell gates hold for >= 95 % (T) / >= 98 % (Y entries) and
+    the rest statistically against the FP64 oracle at rtol 1e-10."""
+    b = _cells(32, seed=5)
+    yo, so = oracle.bdf(MECH, b.state_rows(), b.P, b.dt, threads=8)
+    yt, stt = oracle.bdf(MECH, b.state_rows(), b.P, b.dt, rtol=1e-10, atol=1e-14, threads=8)
+    s = native.Solver(MECH)
+    T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+    st, stats, cnt = s.integrate(T, Y, b.P, b.dt, counters=True)
+    s.close()
+    assert (st == 0).all() and (so["status"] == 0).all() and (stt["status"] == 0).all()
+    assert (T - b.T).max() > 500.0          # ignition happened in the step
+    Yg = Y[:-1].T
+    assert ((np.abs(T - yo[:, 0]) / yo[:, 0]) <= GATE_T).mean() >= 0.95
+    assert y_ok(Yg, yo[:, 1:]).mean() >= 0.98
+    Tt = yt[:, 0]
+    rT = np.abs(T - Tt) / (np.abs(yo[:, 0] - Tt) + 1e-6 * Tt)
+    assert np.quantile(rT, 0.95) <= 2.0 and rT.max() <= 50.0, (np.quantile(rT, 0.95), rT.max())
+    true = yt[:, 1:]
+    frac_gpu = y_ok(Yg, true).mean()
+    frac_cpu = y_ok(yo[:, 1:], true).mean()
+    assert frac_gpu >= frac_cpu - 0.01, (frac_gpu, frac_cpu)
+    ratio = np.abs(Yg - true) / (np.abs(yo[:, 1:] - true) + W.RTOL * np.abs(true) + W.ATOL)
+    assert np.quantile(ratio, 0.99) <= 2.0 and ratio.max() <= 50.0, (np.quantile(ratio, 0.99), ratio.max())
+    assert np.abs(Y.sum(axis=0) - 1.0).max() < 1e-12
+    g, c = cnt["nst"].sum(), so["nst"].sum()
+    assert abs(g - c) <= 0.15 * c + 10, (g, c)
+
+
+def test_persistent_equals_step_form():
+    b = _cells(8, seed=6)
+    out = []
+    for persistent in (1, 0):
+        s = native.Solver(MECH, persistent=persistent)
+        T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+        st, _, _ = s.integrate(T, Y, b.P, b.dt)
+        s.close()
+        out.append((T, Y, st))
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])

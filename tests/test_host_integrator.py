@@ -35,7 +35,9 @@ def test_mechanism_size_mismatch_throws_before_device_work(driver):
     assert rc == 3 and "mechanism size of: gri30.yaml (53) differs from the mesh size: 10" in out
     rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "nDodecane_Reitz.yaml", T, Y, 1e-6, 101325.0)
     assert rc == 3 and "nDodecane_Reitz.yaml (100) differs from the mesh size: 10" in out
-    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "ESTiMatE-Mech_04042022.yaml", T, Y, 1e-6, 101325.0)
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "ESTiMatE-Mech_04042022.xml", T, Y, 1e-6, 101325.0)
+    assert rc == 3 and "ESTiMatE-Mech_04042022.xml (214) differs from the mesh size: 10" in out
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "no_such_mech.yaml", T, Y, 1e-6, 101325.0)
     assert rc == 3 and "(-1) differs" in out
 
 

@@ -18,7 +18,7 @@ needs_ref = pytest.mark.skipif(not os.path.isdir(REF_MECH), reason="reference me
 
 
 @needs_ref
-@pytest.mark.parametrize("name", ["gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004"])
+@pytest.mark.parametrize("name", ["gri30", "h2o2", "nDodecane_Reitz", "h2_li_2004", "ESTiMatE-Mech_04042022"])
 def test_committed_tables_are_generated(tmp_path, name):
     m = M.load(name, REF_MECH)
     out = tmp_path / f"{name}_mech.h"
@@ -55,14 +55,49 @@ def test_h2_grid_workload_reproduces_reference_dataset():
     assert np.abs(b.Y - Y).max() <= 1e-15
 
 
-def test_unsupported_forms_raise(tmp_path):
-    p = tmp_path / "bad.xml"
-    p.write_text("""<ctml><phase id="gas"><speciesArray>A</speciesArray></phase>
+def _ctml(tmp_path, rxn_type, rev, reac, prod):
+    p = tmp_path / "m.xml"
+    p.write_text(f"""<ctml><phase id="gas"><speciesArray>A B</speciesArray></phase>
 <speciesData><species name="A"><atomArray>H:1</atomArray><thermo>
 <NASA Tmin="300" Tmax="1000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA>
+<NASA Tmin="1000" Tmax="5000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA></thermo></species>
+<species name="B"><atomArray>H:2</atomArray><thermo>
+<NASA Tmin="300" Tmax="1000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA>
 <NASA Tmin="1000" Tmax="5000"><floatArray>1,0,0,0,0,0,0</floatArray></NASA></thermo></species></speciesData>
-<reactionData><reaction id="1" type="plog"><equation>A =] A</equation><rateCoeff><Arrhenius><A>1</A><b>0</b>
-<E units="K">0</E></Arrhenius></rateCoeff><reactants>A:1</reactants><products>A:1</products></reaction>
+<reactionData><reaction id="1" reversible="{rev}" type="{rxn_type}"><equation>x</equation><rateCoeff>
+<Arrhenius><A>1</A><b>0</b><E units="K">0</E><P units="atm">1.0</P></Arrhenius></rateCoeff>
+<reactants>{reac}</reactants><products>{prod}</products></reaction>
 </reactionData></ctml>""")
-    with pytest.raises(NotImplementedError):
-        M.Mechanism.from_ctml(str(p), "bad")
+    return str(p)
+
+
+def test_unsupported_forms_raise(tmp_path):
+    with pytest.raises(NotImplementedError):      # Chebyshev rate
+        M.Mechanism.from_ctml(_ctml(tmp_path, "chebyshev", "yes", "A:2", "B:1"), "bad")
+    with pytest.raises(NotImplementedError):      # fractional reactant coefficient
+        M.Mechanism.from_ctml(_ctml(tmp_path, "elementary", "no", "A:1.5", "B:0.75"), "bad")
+    with pytest.raises(NotImplementedError):      # fractional product of a reversible step
+        M.Mechanism.from_ctml(_ctml(tmp_path, "elementary", "yes", "B:1", "A:0.5 B:0.75"), "bad")
+    m = M.Mechanism.from_ctml(_ctml(tmp_path, "elementary", "no", "B:1", "A:1.5 B:0.25"), "ok")
+    assert m.reactions[0].prod == [(0, 1.5), (1, 0.25)]
+    out = tmp_path / "ok_mech.h"
+    m.emit_header(str(out))
+    assert "#define MECH_OK_NU_DEN 4" in open(out).read()
+
+
+@needs_ref
+def test_estimate_mechanism_forms():
+    """ESTiMatE (kerosene, 214 species): PLOG levels sorted by pressure in Pa,
+    lumped irreversible steps with fractional products, tables with NU_DEN 2."""
+    m = M.load("ESTiMatE-Mech_04042022", REF_MECH)
+    c = m.counts()
+    assert (c["species"], c["reactions"], c["plog"], c["troe"], c["lindemann"]) == (214, 1558, 22, 71, 2)
+    plog = [r for r in m.reactions if r.rtype == M.T_PLOG]
+    assert all(r.reversible for r in plog)
+    for r in plog:
+        ps = [p for p, _ in r.plog]
+        assert ps == sorted(ps) and len(set(ps)) == len(ps) and len(ps) >= 2
+    first = plog[0]
+    assert first.equation.startswith("CH3 + OH") and first.plog[0][0] == pytest.approx(0.01 * 101325.0)
+    frac = [r for r in m.reactions if any(v != int(v) for _, v in r.prod)]
+    assert len(frac) == 5 and not any(r.reversible for r in frac)

@@ -55,7 +55,8 @@ def test_jacobian_TT_is_derivative_of_reference_rhs(oracle, golden_chem):
         assert abs(J[0, 0] - fd) <= 1e-5 * max(abs(fd), 1.0), (i, J[0, 0], fd)
 
 
-@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k"), ("nDodecane_Reitz", "nc12_8k")])
+@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k"), ("nDodecane_Reitz", "nc12_8k"),
+                                     ("ESTiMatE-Mech_04042022", "kero_2k")])
 def test_jacobian_finite_difference(oracle, mech, wl):
     b = W.make(wl, 4, seed=7)
     ys = b.state_rows()
@@ -115,3 +116,47 @@ def test_max_steps_cap_and_too_close(oracle):
     assert (st["status"] == -1).all() and (st["nst"] == 5).all()
     y, st = oracle.bdf(b.mech, b.state_rows(), b.P, 0.0)
     assert (st["status"] == -27).all()
+
+
+def _header_arrays(mech):
+    """The generated C header's static arrays, parsed as numpy arrays."""
+    import os
+    import re
+    txt = open(os.path.join(W.MECH_DIR, f"{mech}_mech.h")).read()
+    out = {}
+    for m in re.finditer(r"static const (?:double|int) \w+?_(rxn_\w+|plog_\w+)\[\d+\] = \{([^}]*)\};", txt):
+        out[m.group(1)] = np.array([float(v) for v in m.group(2).split(",")])
+    return out
+
+
+def test_plog_rates_match_log_pressure_interpolation(oracle):
+    """PLOG reactions of the kerosene mechanism: the oracle's k(T, P) against a
+    numpy restatement of the published definition (ln k linear in ln P between
+    the bracketing levels, the end levels' k outside; a level's k is the sum of
+    its Arrhenius terms), below, at, between and above the tabulated pressures."""
+    mech = W.ESTIMATE
+    a = _header_arrays(mech)
+    nr = a["rxn_type"].size
+    off, toff, lnP = a["plog_off"].astype(int), a["plog_term_off"].astype(int), a["plog_lnP"]
+
+    def level(l, T):
+        t = slice(toff[l], toff[l + 1])
+        return np.sum(a["plog_A"][t] * T ** a["plog_b"][t] * np.exp(-a["plog_EaR"][t] / T))
+
+    plog = np.flatnonzero(a["rxn_type"] == 4)
+    assert plog.size == 22
+    for T in (800.0, 1300.0, 2100.0):
+        for P in (0.001 * 101325, 0.01 * 101325, 0.37 * 101325, 1.0 * 101325, 7.5 * 101325, 250 * 101325):
+            kf = oracle.kf(mech, P, T, nr)
+            for r in plog:
+                levels = np.arange(off[r], off[r + 1])
+                lp = np.log(P)
+                if lp <= lnP[levels[0]]:
+                    want = level(levels[0], T)
+                elif lp >= lnP[levels[-1]]:
+                    want = level(levels[-1], T)
+                else:
+                    i = levels[np.searchsorted(lnP[levels], lp) - 1]
+                    w = (lp - lnP[i]) / (lnP[i + 1] - lnP[i])
+                    want = np.exp((1 - w) * np.log(level(i, T)) + w * np.log(level(i + 1, T)))
+                assert kf[r] == pytest.approx(want, rel=1e-12), (r, T, P)
