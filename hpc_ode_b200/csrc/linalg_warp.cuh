@@ -24,23 +24,194 @@ namespace b200 {
 template <class T>
 __device__ __forceinline__ T absT(T v) { return v < T(0) ? -v : v; }
 
-// Factor A in place.  piv[k] = row swapped with row k at step k; perm = the
-// composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
+// LU factorization in place (both forms below give the same factors).  perm =
+// the composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
 // Returns 0, or k+1 if U_kk == 0 (singular).  All 32 lanes call it.
+//
+// Blocked form, in LAPACK's getrf order: a panel of kPanel columns is factored with
+// partial pivoting (full rows swapped), then the panel's block rows right of
+// it are eliminated (U12 = L11^-1 A12) and the trailing matrix gets one
+// rank-kPanel update.  Every element receives the same fused multiply-adds in
+// the same order as in the unblocked right-looking factorization, so the
+// factors are the same; the rank-kPanel update loads and stores each trailing
+// element once per panel instead of once per column.
+//
+// Every loop that stores into A first loads all it needs (registers), then
+// stores: the compiler may not move a load above a store to the same array,
+// so load-store-load chains would wait out the full shared-memory latency
+// once per element (with one warp per SM for the largest mechanisms, nothing
+// else hides it).
 template <class MT, class LinT>
-__device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
-    constexpr int N = MT::N, LDA = MT::LDA;
+__device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    constexpr int kPanel = 4;                               // panel width
+    constexpr int kRows = sizeof(LinT) == 4 ? 8 : 4;        // rows per trailing-update batch
     LinT* A = smem_at<LinT>(A_off);
     int* perm = smem_at<int>(perm_off);
     LinT* dinv = smem_at<LinT>(dinv_off);
-    constexpr int NS = MT::NS;
+    int sing = 0;
+    int pv[NS];   // lane tracks perm[i] for i = lane + 32 s
+#pragma unroll
+    for (int s = 0; s < NS; ++s) pv[s] = lane + 32 * s;
+#pragma unroll 1
+    for (int k0 = 0; k0 < N; k0 += kPanel) {
+        const int kend = min(k0 + kPanel, N);
+        // ---- 1. panel: columns [k0, kend), rows >= k
+#pragma unroll 1
+        for (int k = k0; k < kend; ++k) {
+            // pivot: first index of the max |a_ik|, i >= k
+            LinT best = LinT(-1);
+            int bi = N;
+            for (int i = k + lane; i < N; i += 32) {
+                const LinT v = absT(A[i * LDA + k]);
+                if (v > best) { best = v; bi = i; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const LinT ov = __shfl_xor_sync(kFull, best, o);
+                const int oi = __shfl_xor_sync(kFull, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
+            if (bi != k) {   // swap the full rows k and bi
+                LinT rk[NS], rb[NS];
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const int j = lane + 32 * s;
+                    if (j < N) { rk[s] = A[k * LDA + j]; rb[s] = A[bi * LDA + j]; }
+                }
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    const int j = lane + 32 * s;
+                    if (j < N) { A[k * LDA + j] = rb[s]; A[bi * LDA + j] = rk[s]; }
+                }
+                // compose the permutation: swap entries k and bi
+                const int ok = __shfl_sync(kFull, pick<NS>(pv, k >> 5), k & 31);
+                const int ob = __shfl_sync(kFull, pick<NS>(pv, bi >> 5), bi & 31);
+                if (lane == (k & 31)) place<NS>(pv, k >> 5, ob);
+                if (lane == (bi & 31)) place<NS>(pv, bi >> 5, ok);
+                __syncwarp();
+            }
+            const LinT inv = LinT(1) / A[k * LDA + k];
+            if (lane == 0) dinv[k] = inv;
+            // multipliers (column k below the diagonal), then the panel's
+            // columns right of k; lane owns rows i = k + 1 + lane + 32 t
+            LinT ukj[kPanel - 1];
+#pragma unroll
+            for (int q = 0; q < kPanel - 1; ++q)
+                ukj[q] = (k + 1 + q < kend) ? A[k * LDA + k + 1 + q] : LinT(0);
+#pragma unroll
+            for (int t = 0; t < NS; ++t) {
+                const int i = k + 1 + lane + 32 * t;
+                if (i < N) {
+                    const LinT lik = A[i * LDA + k] * inv;
+                    LinT a[kPanel - 1];
+#pragma unroll
+                    for (int q = 0; q < kPanel - 1; ++q)
+                        if (k + 1 + q < kend) a[q] = A[i * LDA + k + 1 + q];
+                    A[i * LDA + k] = lik;
+#pragma unroll
+                    for (int q = 0; q < kPanel - 1; ++q)
+                        if (k + 1 + q < kend && ukj[q] != LinT(0)) A[i * LDA + k + 1 + q] = a[q] - lik * ukj[q];
+                }
+            }
+            __syncwarp();
+        }
+        if (sing || kend >= N) break;
+        // ---- 2. block rows right of the panel: U12 = L11^-1 A12 (lane owns
+        // columns j = lane + 32 s >= kend; rows in registers)
+        LinT u[kPanel][NS];
+        bool on[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = lane + 32 * s;
+            on[s] = j >= kend && j < N;
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) u[r][s] = (on[s] && k0 + r < kend) ? A[(k0 + r) * LDA + j] : LinT(0);
+        }
+#pragma unroll
+        for (int r = 1; r < kPanel; ++r) {
+            if (k0 + r < kend) {
+#pragma unroll
+                for (int q = 0; q < r; ++q) {
+                    const LinT lrq = A[(k0 + r) * LDA + k0 + q];
+#pragma unroll
+                    for (int s = 0; s < NS; ++s)
+                        if (u[q][s] != LinT(0)) u[r][s] = u[r][s] - lrq * u[q][s];
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = lane + 32 * s;
+            if (on[s]) {
+#pragma unroll
+                for (int r = 1; r < kPanel; ++r)
+                    if (k0 + r < kend) A[(k0 + r) * LDA + j] = u[r][s];
+            }
+            bool nz = false;
+#pragma unroll
+            for (int r = 0; r < kPanel; ++r) nz = nz || (u[r][s] != LinT(0));
+            on[s] = on[s] && nz;   // columns with a zero U12 block need no update
+        }
+        __syncwarp();
+        // ---- 3. trailing update A22 -= L21 U12, rows in batches of kRows
+#pragma unroll 1
+        for (int i0 = kend; i0 < N; i0 += kRows) {
+            const int nr = min(kRows, N - i0);
+            LinT l[kRows][kPanel];
+#pragma unroll
+            for (int rr = 0; rr < kRows; ++rr)
+#pragma unroll
+                for (int q = 0; q < kPanel; ++q)
+                    l[rr][q] = (rr < nr && k0 + q < kend) ? A[(i0 + rr) * LDA + k0 + q] : LinT(0);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                if (on[s]) {
+                    const int j = lane + 32 * s;
+                    LinT a[kRows];
+#pragma unroll
+                    for (int rr = 0; rr < kRows; ++rr)
+                        if (rr < nr) a[rr] = A[(i0 + rr) * LDA + j];
+#pragma unroll
+                    for (int q = 0; q < kPanel; ++q) {
+                        if (u[q][s] != LinT(0)) {
+#pragma unroll
+                            for (int rr = 0; rr < kRows; ++rr) a[rr] = a[rr] - l[rr][q] * u[q][s];
+                        }
+                    }
+#pragma unroll
+                    for (int rr = 0; rr < kRows; ++rr)
+                        if (rr < nr) A[(i0 + rr) * LDA + j] = a[rr];
+                }
+            }
+        }
+        __syncwarp();
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+        if (lane + 32 * s < N) perm[lane + 32 * s] = pv[s];
+    __syncwarp();
+    return sing;
+}
+
+// The unblocked right-looking form of the same factorization (row by row,
+// one rank-1 update per column): the smallest code.  With several warps per
+// SM the latency it exposes is hidden by the other warps, and the kernels of
+// the small mechanisms are bound by instruction fetch, where the blocked
+// form's larger code costs more than it saves.
+template <class MT, class LinT>
+__device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    LinT* A = smem_at<LinT>(A_off);
+    int* perm = smem_at<int>(perm_off);
+    LinT* dinv = smem_at<LinT>(dinv_off);
     int sing = 0;
     int pv[NS];   // lane tracks perm[i] for i = lane + 32 s
 #pragma unroll
     for (int s = 0; s < NS; ++s) pv[s] = lane + 32 * s;
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
-        // pivot: first index of the max |a_ik|, i >= k
         LinT best = LinT(-1);
         int bi = N;
         for (int i = k + lane; i < N; i += 32) {
@@ -61,7 +232,6 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
                 A[k * LDA + j] = A[bi * LDA + j];
                 A[bi * LDA + j] = t;
             }
-            // compose the permutation: swap entries k and bi
             const int ok = __shfl_sync(kFull, pick<NS>(pv, k >> 5), k & 31);
             const int ob = __shfl_sync(kFull, pick<NS>(pv, bi >> 5), bi & 31);
             if (lane == (k & 31)) place<NS>(pv, k >> 5, ob);
@@ -87,6 +257,15 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
         if (lane + 32 * s < N) perm[lane + 32 * s] = pv[s];
     __syncwarp();
     return sing;
+}
+
+// Matrices from this size up (one to four warps per SM) take the blocked form.
+constexpr int kBlockedLuMinN = 96;
+
+template <class MT, class LinT>
+__device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+    if constexpr (MT::N >= kBlockedLuMinN) return warp_lu_blocked<MT, LinT>(A_off, perm_off, dinv_off, lane);
+    else return warp_lu_compact<MT, LinT>(A_off, perm_off, dinv_off, lane);
 }
 
 // Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + 32 s) in,
