@@ -107,17 +107,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(batch: W.Batch, ncells: int, threads: int):
+def cpu_reference(batch: W.Batch, ncells: int, threads: int, conv: bool = False):
     """Time the reference-semantics CPU integrator on a stratified sample."""
     from oracle import pyoracle
     o = pyoracle.get()
     stride = max(1, batch.ncells // ncells)
     idx = np.arange(0, batch.ncells, stride)[:ncells]
     sub = batch.subset(idx)
-    use_ref = o.has_ref() and batch.mech == "gri30"
+    use_ref = o.has_ref() and batch.mech == "gri30" and not conv   # the reference pyJac is CONP
     t0 = time.perf_counter()
     _, st = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=W.RTOL, atol=W.ATOL,
-                  threads=threads, use_ref_kernels=use_ref)
+                  threads=threads, use_ref_kernels=use_ref, conv=conv)
     el = time.perf_counter() - t0
     kind = "reference" if use_ref else "port"
     what = ("CVODE-semantics BDF (oracle/bdf_oracle.c) + reference pyJac C RHS/Jacobian"
@@ -132,13 +132,14 @@ def run_reference_arm(args):
     batch = W.make(args.workload)
     threads = os.cpu_count() or 1
     sample = args.cpu_sample
+    conv = args.formulation == "conv"
     for _ in range(args.warmup):
-        cpu_reference(batch, max(64, sample // 8), threads)
+        cpu_reference(batch, max(64, sample // 8), threads, conv=conv)
     times = []
     n_done = 0
     kind = what = None
     for _ in range(args.steps):
-        n, el, kind, what, _ = cpu_reference(batch, sample, threads)
+        n, el, kind, what, _ = cpu_reference(batch, sample, threads, conv=conv)
         times.append(el)
         n_done += n
     total = sum(times)
@@ -159,7 +160,8 @@ def run_reference_arm(args):
     return 0
 
 
-def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample: int = 256) -> dict:
+def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample: int = 256,
+                   conv: bool = False) -> dict:
     """Error of the GPU result against the FP64 oracle (the CVODE-semantics BDF
     at rtol 1e-10 / atol 1e-14) on a stratified sample of cells, beside the
     error of the CPU integrator at the same rtol/atol as the GPU."""
@@ -169,8 +171,10 @@ def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample
     idx = np.arange(0, n, max(1, n // nsample))[:nsample]
     sub = batch.subset(idx)
     threads = os.cpu_count() or 1
-    ytrue, st_true = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=1e-10, atol=1e-14, threads=threads)
-    ycpu, _ = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=W.RTOL, atol=W.ATOL, threads=threads)
+    ytrue, st_true = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=1e-10, atol=1e-14, threads=threads,
+                           conv=conv)
+    ycpu, _ = o.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, rtol=W.RTOL, atol=W.ATOL, threads=threads,
+                    conv=conv)
     Tg, Yg = T_gpu[idx], Y_gpu[:-1, idx].T
     eT = np.abs(Tg - ytrue[:, 0]) / ytrue[:, 0]
     eTc = np.abs(ycpu[:, 0] - ytrue[:, 0]) / ytrue[:, 0]
@@ -260,6 +264,8 @@ def main():
     ap.add_argument("--ncells", type=int, default=None, help="override cells per GPU")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--form", default="persistent", choices=["persistent", "step"])
+    ap.add_argument("--formulation", default="conp", choices=["conp", "conv"],
+                    help="constant pressure (the reference's) or constant volume")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=8192,
                     help="cells of the workload the CPU baseline integrates per step (stratified)")
@@ -291,8 +297,9 @@ def main():
     n = args.ncells or cfg["ncells"]
     batch = W.make(args.workload, n, seed=cfg["seed"] + 1000 * rank)
     prec = native.B200ODE_MIXED if args.precision == "mixed" else native.B200ODE_FP64
+    form = native.B200ODE_CONV if args.formulation == "conv" else native.B200ODE_CONP
     solver = native.Solver(batch.mech, precision=prec, persistent=int(args.form == "persistent"),
-                           device=dev.index)
+                           device=dev.index, formulation=form)
     nsp = solver.nsp
     T0 = torch.from_numpy(batch.T).to(dev)
     Y0 = torch.from_numpy(np.ascontiguousarray(batch.Y)).to(dev)
@@ -427,7 +434,8 @@ def main():
     ref = None
     if not args.no_fp64_step and args.precision == "mixed" and args.form == "persistent":
         try:
-            ref = native.Solver(batch.mech, precision=native.B200ODE_FP64, persistent=0, device=dev.index)
+            ref = native.Solver(batch.mech, precision=native.B200ODE_FP64, persistent=0, device=dev.index,
+                                formulation=form)
         except native.B200Error as e:   # e.g. a Newton matrix too large for FP64 in shared memory
             fp64_step = {"unavailable": str(e)}
     if ref is not None:
@@ -463,13 +471,14 @@ def main():
     acc = None
     if rank == 0 and not args.no_accuracy:
         try:
-            acc = accuracy_block(batch, T.cpu().numpy(), Y.cpu().numpy())
+            acc = accuracy_block(batch, T.cpu().numpy(), Y.cpu().numpy(), conv=args.formulation == "conv")
         except Exception as e:  # noqa: BLE001
             acc = {"error": str(e)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        ncpu, el, kind, what, _ = cpu_reference(batch, args.cpu_sample, os.cpu_count() or 1)
+        ncpu, el, kind, what, _ = cpu_reference(batch, args.cpu_sample, os.cpu_count() or 1,
+                                                conv=args.formulation == "conv")
         cpu = {"value": ncpu / el, "unit": "cells/s", "cores": os.cpu_count() or 1, "kind": kind,
                "sample": f"{ncpu} of {n} cells (every {max(1, n // ncpu)}th), {what}"}
 
@@ -481,7 +490,7 @@ def main():
         "data": "synthetic (seeded; stands in for the reference's missing 55,076-cell flame dataset)",
         "config": {"workload": args.workload, "mechanism": batch.mech, "cells_per_gpu": n,
                    "dt": batch.dt, "rtol": W.RTOL, "atol": W.ATOL,
-                   "precision": args.precision, "form": args.form,
+                   "precision": args.precision, "form": args.form, "formulation": args.formulation,
                    "l2": "256 MiB memset between timed steps (inputs smaller than L2)",
                    "parallelism": f"cell shards x{ws}, no collective"},
         "kernel_ms_per_step": kernel_ms,

@@ -124,6 +124,7 @@ struct KParams {
     double t0, t1, rtol, atol;
     int max_steps, max_order, refine, steps;
     int chunk;                        // persistent form: cells a warp claims per queue access
+    int conv;                         // constant volume: P is each cell's initial pressure
 };
 
 template <class MT>
@@ -136,6 +137,38 @@ __device__ __forceinline__ void load_cell(const KParams& p, long long cell, int 
         else if (i == N - 1) y0[s] = p.T[cell];
         else y0[s] = 0.0;
     }
+}
+
+// Density P W / (R T) of a cell's state at pressure P; y in internal order
+// [Y_0 .. Y_{N-2}, T].  In the constant-volume form the kernels carry -rho
+// in the pressure slot (the chemistry then takes rho as fixed, see
+// species_phase).
+template <class MT>
+__device__ __forceinline__ double cell_density(double P, const double (&y)[MT::NS], int lane) {
+    constexpr int N = MT::N;
+    const DevMech& M = mech<MT>();
+    double sy = 0.0, sw = 0.0;
+#pragma unroll
+    for (int s = 0; s < MT::NS; ++s) {
+        const int i = lane + 32 * s;
+        if (i < N - 1) {
+            sy += y[s];
+            sw += y[s] * __ldg(M.inv_mw + i);
+        }
+    }
+    sy = warp_sum(sy);
+    sw = warp_sum(sw) + (1.0 - sy) * __ldg(M.inv_mw + N - 1);
+    const double T = __shfl_sync(kFull, y[(N - 1) / 32], (N - 1) % 32);
+    return ode_div(P, kRU * T * sw);
+}
+
+// The value the chemistry takes in its pressure slot: P (constant pressure) or
+// -rho of the state at P (constant volume).
+template <class MT>
+__device__ __forceinline__ double pressure_slot(const KParams& p, long long cell, const double (&y)[MT::NS],
+                                                int lane) {
+    const double P = p.P ? p.P[cell] : p.P_scalar;
+    return p.conv ? -cell_density<MT>(P, y, lane) : P;
 }
 
 template <class MT>
@@ -220,7 +253,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         if (phase == 0) {
             Vec<MT::NS> y0;
             load_cell<MT>(p, cell, lane, y0.v);
-            S.P = p.P ? p.P[cell] : p.P_scalar;
+            S.P = pressure_slot<MT>(p, cell, y0.v, lane);
             status = bdf_begin<MT, LinT>(off, y0, p.t0, p.t1, lane);
             done = (status != 0);
         }
@@ -260,7 +293,7 @@ __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParam
     auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     Vec<MT::NS> y;
     load_cell<MT>(p, cell, lane, y.v);
-    const double P = p.P ? p.P[cell] : p.P_scalar;
+    const double P = pressure_slot<MT>(p, cell, y.v, lane);
     const Vec<MT::NS> f = warp_rhs<MT>(P, y, smem_off(&sm->chem), lane);
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
@@ -280,7 +313,7 @@ __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParam
     auto* wg = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal) + cell;
     Vec<MT::NS> y;
     load_cell<MT>(p, cell, lane, y.v);
-    const double P = p.P ? p.P[cell] : p.P_scalar;
+    const double P = pressure_slot<MT>(p, cell, y.v, lane);
     warp_jac<MT, LinT>(P, y, smem_off(sm->A), smem_off(&sm->chem), &wg->js, lane);
     constexpr int N = MT::N;
     double* out = jac + cell * (long long)(N * N);
@@ -558,6 +591,7 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
     p.max_order = h->opt.max_order;
     p.refine = h->opt.refine;
     p.chunk = std::max(1, std::min(h->opt.queue_chunk, 64));
+    p.conv = h->opt.formulation == B200ODE_CONV;
 }
 
 b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {
@@ -643,6 +677,7 @@ void b200ode_default_options(b200ode_options* o) {
     o->use_graph = 0;
     o->device = -1;
     o->profile_phases = 0;
+    o->formulation = B200ODE_CONP;
 }
 
 const char* b200ode_last_error(void) { return g_last_error.c_str(); }
@@ -680,6 +715,8 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
     if (o.max_order < 1 || o.max_order > 5) o.max_order = 5;
     if (o.precision != B200ODE_FP64 && o.precision != B200ODE_MIXED)
         return fail(B200ODE_ERR_INVALID, "precision must be B200ODE_FP64 or B200ODE_MIXED");
+    if (o.formulation != B200ODE_CONP && o.formulation != B200ODE_CONV)
+        return fail(B200ODE_ERR_INVALID, "formulation must be B200ODE_CONP or B200ODE_CONV");
     if (mech == MECH_ESTIMATE && o.precision == B200ODE_FP64)
         return fail(B200ODE_ERR_INVALID,
                     "ESTiMatE-Mech_04042022 (214 unknowns) runs in B200ODE_MIXED only: its FP64 Newton "

@@ -180,8 +180,15 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     c.mw_avg = ode_div(1.0, warp_sum(sw));
     c.logT = log(c.T);
     c.invT = ode_div(1.0, c.T);
-    c.rho = ode_div(P * c.mw_avg, kRU * c.T);
-    c.m = ode_div(P, kRU * c.T);
+    // P >= 0: constant pressure P.  P < 0: constant volume, -P is the cell's
+    // fixed density and the pressure follows from the state (P = rho R T / W).
+    if (P >= 0.0) {
+        c.rho = ode_div(P * c.mw_avg, kRU * c.T);
+        c.m = ode_div(P, kRU * c.T);
+    } else {
+        c.rho = -P;
+        c.m = ode_div(-P, c.mw_avg);
+    }
     double csum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
@@ -284,7 +291,7 @@ __device__ __noinline__ FallOut falloff(int s, int fl, double T, double logT, do
 // reference's Cantera integrator evaluates for these reactions); a level's k
 // is the sum of its Arrhenius terms.  Returns ln k and d ln k / dT.
 struct PlogOut {
-    double lnk, dlnk_dT;
+    double lnk, dlnk_dT, dlnk_dlnP;   // d ln k / d ln P: 0 outside the table
 };
 
 template <class MT>
@@ -318,7 +325,8 @@ __device__ __noinline__ PlogOut plog_rate(int s, double T, double logT, double i
         lk[e] = ode_log(k);
         dl[e] = ode_div(dk, k);
     }
-    return PlogOut{(1.0 - w) * lk[0] + w * lk[1], (1.0 - w) * dl[0] + w * dl[1]};
+    const double slope = (hi != lo) ? ode_div(lk[1] - lk[0], __ldg(M.plog_lnP + hi) - __ldg(M.plog_lnP + lo)) : 0.0;
+    return PlogOut{(1.0 - w) * lk[0] + w * lk[1], (1.0 - w) * dl[0] + w * dl[1], slope};
 }
 
 // Cell quantities the reaction phase needs (passed by value to the
@@ -458,17 +466,20 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) om[s] = g.v[s];
     }
+    // energy equation: enthalpy and cp at constant pressure; internal energy
+    // u = h - R T / W_k and cv = cp - R / W_k at constant volume (P < 0)
+    const double one = (P < 0.0) ? 1.0 : 0.0;
     double qsum = 0.0, cpsum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
         const int i = lane + 32 * s;
         if (i < N) {
-            qsum += om[s] * hRT[s];
-            cpsum += cpR[s] * Yk[s] * __ldg(M.inv_mw + i);
+            qsum += om[s] * (hRT[s] - one);
+            cpsum += (cpR[s] - one) * Yk[s] * __ldg(M.inv_mw + i);
         }
     }
-    const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k h_k W_k   [W/m^3]
-    const double cp_avg = kRU * warp_sum(cpsum);           // [J/kg/K]
+    const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k e_k W_k   [W/m^3]
+    const double cp_avg = kRU * warp_sum(cpsum);           // cp or cv [J/kg/K]
     const double dTdt = ode_div(-Q, c.rho * cp_avg);
     const double inv_rho = ode_div(1.0, c.rho);
     Vec<MT::NS> fv;
@@ -485,7 +496,11 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 
 // Analytic Jacobian J = d f / d y (internal order) into A (row-major, lda MT::LDA),
 // in precision LinT.  Chain rule through concentrations and the closure species:
-//   dC_i/dY_j = rho/W_i (delta_ij - delta_{i,N-1}) - C_i Wbar (1/W_j - 1/W_{N-1}).
+//   dC_i/dY_j = rho/W_i (delta_ij - delta_{i,N-1}) - C_i Wbar (1/W_j - 1/W_{N-1})
+// at constant pressure (rho = P Wbar / (R T)); at constant volume (P < 0, rho
+// fixed) the second term is absent, C does not depend on T, and the total
+// concentration m = sum_i C_i (third bodies, PLOG pressure) adds
+// dw/dm (1/W_j - 1/W_{N-1}) rho to every column.
 // d q / d C_j is scattered into the species-space rows with shared-memory
 // atomics (one warp per cell, so the accumulation never leaves the warp).
 template <class MT, class LinT>
@@ -502,6 +517,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
 #pragma unroll 2
     for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
+    const bool conv = P < 0.0;   // constant volume (see species_phase)
     constexpr int ns = MT::NSLOT;
     const RxnCtx rc = rxn_ctx(c);
     const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
@@ -537,8 +553,23 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             for (int a = 0; a < 3; ++a) { ordf += (rf[a] < N); ordr += (pf[a] < N); }
             const double Sr = o.phi * (ordf * o.Rf - ordr * o.Rr);
             thd_term = R * o.dphi_dthd;
-            dqdT = o.phi * dR_dT + R * o.dphi_dT - (Sr + thd_term * o.thd) * c.invT;
-            sr = Sr + thd_term * (o.thd - c.m);
+            if (!conv) {
+                // C = rho Y / W with rho = P W / (R T): C and m fall as 1/T
+                dqdT = o.phi * dR_dT + R * o.dphi_dT - (Sr + thd_term * o.thd) * c.invT;
+                sr = Sr + thd_term * (o.thd - c.m);          // sum_i dq/dC_i C_i
+            } else {
+                // C fixed in T; m = sum_i C_i, and P = m R T moves PLOG rates
+                // with T and with every C_i: sr = dq/dm
+                dqdT = o.phi * dR_dT + R * o.dphi_dT;
+                sr = thd_term;
+                if constexpr (MT::PLOG) {
+                    if (fl & kFlagPlog) {
+                        const PlogOut pl = plog_rate<MT>(s, c.T, c.logT, c.invT, ode_log(c.m * kRU * c.T));
+                        dqdT += o.q * pl.dlnk_dlnP * c.invT;
+                        sr += ode_div(o.q * pl.dlnk_dlnP, c.m);
+                    }
+                }
+            }
             const double* C = sm->C;
             dRf[0] = o.phi * o.kf * (C[rf[1]] * C[rf[2]]);
             dRf[1] = o.phi * o.kf * (C[rf[0]] * C[rf[2]]);
@@ -600,11 +631,15 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             const double Wi = __ldg(M.mw + i), iWi = __ldg(M.inv_mw + i);
             const double Wr = Wi * inv_rho;
             const double fk = w[s] * Wr;
-            dfdT[s] = Wr * (dw[s] + w[s] * c.invT);
-            const double hW = RT * hRT[s];                 // h_k W_k  [J/kmol]
+            // constant pressure: energy h, heat capacity cp, f = w W / rho(T, Y);
+            // constant volume: u = h - R T / W_k, cv = cp - R / W_k, rho fixed,
+            // and sk holds dw/dm (m = sum_i C_i) instead of sum_i dw/dC_i C_i
+            const double one = conv ? 1.0 : 0.0;
+            dfdT[s] = Wr * (dw[s] + (conv ? 0.0 : w[s] * c.invT));
+            const double hW = RT * (hRT[s] - one);         // e_k W_k  [J/kmol]
             const double hk = hW * iWi;                    // J/kg
-            const double cpk = kRU * cpR[s] * iWi;         // J/kg/K
-            const double X = (c.mw_avg * inv_rho) * (w[s] - sk[s]);
+            const double cpk = kRU * (cpR[s] - one) * iWi; // J/kg/K
+            const double X = conv ? sk[s] : (c.mw_avg * inv_rho) * (w[s] - sk[s]);
             spw[0 * N + i] = hW;
             spw[1 * N + i] = cpk;
             spw[2 * N + i] = X;

@@ -56,7 +56,9 @@ int cfg_int(const std::string& key, const std::string& v) {
 
 // Applies the b200 options of the config: precision (fp64 | mixed), refine (0 | 1),
 // max_steps, max_order, form (persistent | step), graph (0 | 1), warps_per_block,
-// blocks_per_sm, device, enthalpy (keep | update).  Unknown values throw
+// blocks_per_sm, device, enthalpy (keep | update), formulation (conp | conv:
+// constant volume, the config's pressure then being each cell's initial
+// pressure).  Unknown values throw
 // std::runtime_error.
 void apply_config(const IntegratorConfig& c, b200ode_options* o, bool* update_enthalpy) {
     std::string v;
@@ -69,6 +71,11 @@ void apply_config(const IntegratorConfig& c, b200ode_options* o, bool* update_en
         if (v == "fp64") o->precision = B200ODE_FP64;
         else if (v == "mixed") o->precision = B200ODE_MIXED;
         else throw std::runtime_error("b200.precision must be fp64 or mixed, not '" + v + "'");
+    }
+    if (cfg_get(c, "formulation", &v)) {
+        if (v == "conp") o->formulation = B200ODE_CONP;
+        else if (v == "conv") o->formulation = B200ODE_CONV;
+        else throw std::runtime_error("b200.formulation must be conp or conv, not '" + v + "'");
     }
     if (cfg_get(c, "form", &v)) {
         if (v == "persistent") o->persistent = 1;

@@ -17,6 +17,8 @@ LIB_PATH = os.path.join(PKG, "libb200ode.so")
 B200ODE_OK = 0
 B200ODE_FP64 = 0
 B200ODE_MIXED = 1
+B200ODE_CONP = 0
+B200ODE_CONV = 1
 STATUS_NAMES = {0: "OK", 1: "ERR_INVALID", 2: "ERR_MECHANISM", 3: "ERR_CUDA", 4: "ERR_ALLOC",
                 5: "ERR_NO_DEVICE", 6: "ERR_BUSY", 7: "ERR_NOT_READY"}
 CELL_STATUS = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC",
@@ -49,7 +51,8 @@ class Options(C.Structure):
                 ("max_order", C.c_int32), ("precision", C.c_int32), ("refine", C.c_int32),
                 ("persistent", C.c_int32), ("warps_per_block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("queue_chunk", C.c_int32),
-                ("use_graph", C.c_int32), ("device", C.c_int32), ("profile_phases", C.c_int32)]
+                ("use_graph", C.c_int32), ("device", C.c_int32), ("profile_phases", C.c_int32),
+                ("formulation", C.c_int32)]
 
 
 _i32p = C.POINTER(C.c_int32)

@@ -57,6 +57,15 @@ enum {
 
 typedef enum { B200ODE_FP64 = 0, B200ODE_MIXED = 1 } b200ode_precision;
 
+/* Reactor formulation.  CONP: constant pressure (the reference's pyJac build,
+ * src/Mechanism/CPU/dydt.c:7-133): P per cell is held, enthalpy conserved.
+ * CONV: constant volume (pyJac's CONV branch, dydt.c:135-265, which the
+ * reference ships but does not compile): the P given per cell is the initial
+ * pressure, the cell's density rho = P W / (R T) of its initial state is held,
+ * the pressure follows the state (P = rho R T / W) and internal energy is
+ * conserved. */
+typedef enum { B200ODE_CONP = 0, B200ODE_CONV = 1 } b200ode_formulation;
+
 typedef struct {
     double reltol;            /* CVodeSStolerances reltol (reference: 1e-6) */
     double abstol;            /* CVodeSStolerances abstol (reference: 1e-10) */
@@ -73,6 +82,7 @@ typedef struct {
     int32_t use_graph;        /* one-launch-per-step form: capture the step launches in a CUDA graph */
     int32_t device;           /* CUDA device ordinal (-1 = current) */
     int32_t profile_phases;   /* 1 = accumulate per-phase device cycles into b200ode_stats */
+    int32_t formulation;      /* B200ODE_CONP (default) or B200ODE_CONV */
 } b200ode_options;
 
 /* Optional per-cell counters (CVodeGetNum* equivalents) and call totals.  Any

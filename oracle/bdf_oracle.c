@@ -655,14 +655,25 @@ long oracle_bdf_batch(oracle_rhs_fn f, oracle_jac_fn J, int n, long ncells, cons
 long oracle_bdf_batch_mech(int mech, long ncells, const double* pres, double pres_scalar,
                            double* y, double t0, double tout, const oracle_bdf_opts* opts,
                            oracle_bdf_stats* stats, int nthreads) {
-    oracle_rhs_fn f = mech == ORACLE_MECH_GRI30 ? oracle_gri30_dydt
-                      : mech == ORACLE_MECH_H2O2 ? oracle_h2o2_dydt
-                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_dydt
-                      : mech == ORACLE_MECH_ESTIMATE ? oracle_estimate_dydt : oracle_ndodecane_dydt;
-    oracle_jac_fn J = mech == ORACLE_MECH_GRI30 ? oracle_gri30_jacob
-                      : mech == ORACLE_MECH_H2O2 ? oracle_h2o2_jacob
-                      : mech == ORACLE_MECH_H2LI ? oracle_h2li_jacob
-                      : mech == ORACLE_MECH_ESTIMATE ? oracle_estimate_jacob : oracle_ndodecane_jacob;
+    oracle_rhs_fn f;
+    oracle_jac_fn J;
+    oracle_mech_fns(mech, 0, &f, &J);
     return oracle_bdf_batch(f, J, oracle_mech_nsp(mech), ncells, pres, pres_scalar, y, t0, tout,
                             opts, stats, nthreads);
+}
+
+long oracle_bdf_batch_mech_conv(int mech, long ncells, const double* pres, double pres_scalar,
+                                double* y, double t0, double tout, const oracle_bdf_opts* opts,
+                                oracle_bdf_stats* stats, int nthreads) {
+    oracle_rhs_fn f;
+    oracle_jac_fn J;
+    oracle_mech_fns(mech, 1, &f, &J);
+    const int n = oracle_mech_nsp(mech);
+    double* rho = (double*)malloc((size_t)(ncells > 0 ? ncells : 1) * sizeof(double));
+    if (!rho) return ncells;
+    for (long c = 0; c < ncells; ++c)
+        rho[c] = oracle_density(mech, pres ? pres[c] : pres_scalar, y + (size_t)c * n);
+    const long nfail = oracle_bdf_batch(f, J, n, ncells, rho, 0.0, y, t0, tout, opts, stats, nthreads);
+    free(rho);
+    return nfail;
 }

@@ -79,6 +79,16 @@ long oracle_bdf_batch_mech(int mech, long ncells, const double* pres, double pre
                            double* y, double t0, double tout, const oracle_bdf_opts* opts,
                            oracle_bdf_stats* stats, int nthreads);
 
+/* Constant-volume form: pres (or pres_scalar) is each cell's initial
+ * pressure; the cell's density follows from its initial state and stays fixed. */
+long oracle_bdf_batch_mech_conv(int mech, long ncells, const double* pres, double pres_scalar,
+                                double* y, double t0, double tout, const oracle_bdf_opts* opts,
+                                oracle_bdf_stats* stats, int nthreads);
+
+/* The chemistry callbacks of a mechanism id (conv = 1: constant volume, the
+ * pres argument carrying the density). */
+void oracle_mech_fns(int mech, int conv, oracle_rhs_fn* f, oracle_jac_fn* J);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@
  * layout; it agrees with pyJac's to round-off.
  */
 #include "chem_oracle.h"
+#include "bdf_oracle.h"
 
 #include <math.h>
 #include <string.h>
@@ -110,6 +111,7 @@ typedef struct {
     double dphi_dthd;     /* d phi / d thd at fixed T */
     double dphi_dT;       /* d phi / d T at fixed thd */
     double dlnkf_dT, dlnkr_dT;
+    double dlnk_dlnP;     /* PLOG: d ln k / d ln P at fixed T (0 otherwise) */
     int ordf, ordr;
 } rxn_eval_t;
 
@@ -132,7 +134,8 @@ static double plog_level(const mech_t* M, int l, double T, double logT, double* 
 
 /* PLOG rate of reaction r at (T, P): ln k linear in ln P between the levels
  * that bracket P, the end level's k outside their range. */
-static double plog_rate(const mech_t* M, int r, double T, double logT, double lnP, double* dlnk_dT) {
+static double plog_rate(const mech_t* M, int r, double T, double logT, double lnP, double* dlnk_dT,
+                        double* dlnk_dlnP) {
     const int l0 = M->plog_off[r], l1 = M->plog_off[r + 1] - 1;
     int lo = l0, hi = l0;
     double w = 0.0;
@@ -147,15 +150,17 @@ static double plog_rate(const mech_t* M, int r, double T, double logT, double ln
     const double k0 = plog_level(M, lo, T, logT, &d0);
     const double k1 = plog_level(M, hi, T, logT, &d1);
     *dlnk_dT = (1.0 - w) * d0 + w * d1;
+    *dlnk_dlnP = hi != lo ? (log(k1) - log(k0)) / (M->plog_lnP[hi] - M->plog_lnP[lo]) : 0.0;
     return exp((1.0 - w) * log(k0) + w * log(k1));
 }
 
 static void eval_reaction(const mech_t* M, int r, double T, double logT, double m,
                           const double* C, const double* mgRT, int want_deriv, rxn_eval_t* o) {
     const int P = M->maxp;
-    double dlnkf_dT = (M->b[r] + M->EaR[r] / T) / T;
-    double kf = M->type[r] == 4 ? plog_rate(M, r, T, logT, log(m * RU * T), &dlnkf_dT)
+    double dlnkf_dT = (M->b[r] + M->EaR[r] / T) / T, dlnk_dlnP = 0.0;
+    double kf = M->type[r] == 4 ? plog_rate(M, r, T, logT, log(m * RU * T), &dlnkf_dT, &dlnk_dlnP)
                                 : arrh(M->A[r], M->logA[r], M->b[r], M->EaR[r], logT, T);
+    o->dlnk_dlnP = dlnk_dlnP;
     double Rf = 1.0, Rr = 1.0;
     int ordf = 0, ordr = 0, dnu = 0;
     double sum_g = 0.0;
@@ -256,7 +261,10 @@ typedef struct {
     double omega[MAXNSP];
 } state_t;
 
-static void eval_state(const mech_t* M, double pres, const double* y, state_t* s) {
+/* Cell state.  Constant pressure (conv = 0): pres is P.  Constant volume
+ * (conv = 1): pres is the cell's fixed density rho, and the pressure follows
+ * from the state, P = rho R T / W (so m = rho / W). */
+static void eval_state(const mech_t* M, double pres, int conv, const double* y, state_t* s) {
     const int n = M->nsp;
     s->T = y[0];
     s->logT = log(s->T);
@@ -267,9 +275,9 @@ static void eval_state(const mech_t* M, double pres, const double* y, state_t* s
     double inv = 0.0;
     for (int k = 0; k < n; ++k) inv += s->Y[k] * (1.0 / M->mw[k]);
     s->mw_avg = 1.0 / inv;
-    s->rho = pres * s->mw_avg / (RU * s->T);
+    s->rho = conv ? pres : pres * s->mw_avg / (RU * s->T);
     for (int k = 0; k < n; ++k) s->C[k] = s->rho * s->Y[k] * (1.0 / M->mw[k]);
-    s->m = pres / (RU * s->T);
+    s->m = conv ? pres / s->mw_avg : pres / (RU * s->T);
     s->cp_avg = 0.0;
     for (int k = 0; k < n; ++k) {
         const double* a = nasa(M, k, s->T);
@@ -295,7 +303,10 @@ static void add_stoich(const mech_t* M, int r, double q, double* acc) {
     }
 }
 
-static void rhs_from_state(const mech_t* M, state_t* s, double* dy, double* scale) {
+/* dT/dt = -sum_k e_k W_k omega_k / (rho c), e = h, c = cp at constant
+ * pressure; e = u = h - R T / W_k, c = cv = cp - R / W at constant volume
+ * (closed adiabatic reactor: enthalpy, resp. internal energy, conserved). */
+static void rhs_from_state(const mech_t* M, state_t* s, int conv, double* dy, double* scale) {
     const int n = M->nsp;
     double absacc[MAXNSP];
     memset(s->omega, 0, sizeof(double) * n);
@@ -314,13 +325,15 @@ static void rhs_from_state(const mech_t* M, state_t* s, double* dy, double* scal
     }
     double Q = 0.0, Qa = 0.0;
     for (int k = 0; k < n; ++k) {
-        Q += s->omega[k] * s->h[k] * M->mw[k];
-        Qa += absacc[k] * fabs(s->h[k]) * M->mw[k];
+        const double e = conv ? s->h[k] - RU * s->T / M->mw[k] : s->h[k];
+        Q += s->omega[k] * e * M->mw[k];
+        Qa += absacc[k] * fabs(e) * M->mw[k];
     }
-    dy[0] = (-1.0 / (s->rho * s->cp_avg)) * Q;
+    const double c = conv ? s->cp_avg - RU / s->mw_avg : s->cp_avg;
+    dy[0] = (-1.0 / (s->rho * c)) * Q;
     for (int k = 0; k < n - 1; ++k) dy[k + 1] = s->omega[k] * (M->mw[k] / s->rho);
     if (scale) {
-        scale[0] = Qa / (s->rho * s->cp_avg);
+        scale[0] = Qa / (s->rho * c);
         for (int k = 0; k < n - 1; ++k) scale[k + 1] = absacc[k] * (M->mw[k] / s->rho);
     }
 }
@@ -328,16 +341,38 @@ static void rhs_from_state(const mech_t* M, state_t* s, double* dy, double* scal
 void oracle_dydt(int mech, double pres, const double* y, double* dy) {
     const mech_t* M = &MECHS[mech];
     state_t s;
-    eval_state(M, pres, y, &s);
-    rhs_from_state(M, &s, dy, NULL);
+    eval_state(M, pres, 0, y, &s);
+    rhs_from_state(M, &s, 0, dy, NULL);
+}
+
+void oracle_dydt_conv(int mech, double rho, const double* y, double* dy) {
+    const mech_t* M = &MECHS[mech];
+    state_t s;
+    eval_state(M, rho, 1, y, &s);
+    rhs_from_state(M, &s, 1, dy, NULL);
+}
+
+double oracle_density(int mech, double pres, const double* y) {
+    const mech_t* M = &MECHS[mech];
+    state_t s;
+    eval_state(M, pres, 0, y, &s);
+    return s.rho;
 }
 
 void oracle_dydt_scale(int mech, double pres, const double* y, double* scale) {
     const mech_t* M = &MECHS[mech];
     state_t s;
     double dy[MAXNSP];
-    eval_state(M, pres, y, &s);
-    rhs_from_state(M, &s, dy, scale);
+    eval_state(M, pres, 0, y, &s);
+    rhs_from_state(M, &s, 0, dy, scale);
+}
+
+void oracle_dydt_scale_conv(int mech, double rho, const double* y, double* scale) {
+    const mech_t* M = &MECHS[mech];
+    state_t s;
+    double dy[MAXNSP];
+    eval_state(M, rho, 1, y, &s);
+    rhs_from_state(M, &s, 1, dy, scale);
 }
 
 /* -------------------------------------------------------------- Jacobian */
@@ -348,11 +383,16 @@ static double stoich(const mech_t* M, int side, int e) {
     return side ? M->prod_nu[e] : (double)M->reac_nu[e];
 }
 
-void oracle_jacob(int mech, double pres, const double* y, double* jac) {
+/* Exact Jacobian of rhs_from_state.  Constant pressure: C_k = rho(Y, T) Y_k / W_k
+ * with rho = P W / (R T) and m = P / (R T).  Constant volume: rho fixed,
+ * m = sum_k C_k, P = m R T, so C and m do not depend on T, the third-body
+ * concentration and the PLOG pressure depend on every C_i (g_k below), and the
+ * energy equation uses u and cv. */
+static void jacob_impl(int mech, double pres, int conv, const double* y, double* jac) {
     const mech_t* M = &MECHS[mech];
     const int n = M->nsp, P = M->maxp;
     state_t s;
-    eval_state(M, pres, y, &s);
+    eval_state(M, pres, conv, y, &s);
     const double T = s.T;
     /* Jc[k][i] = d omega_k / d C_i (dense, closure column/row included) */
     double* Jc = (double*)calloc((size_t)n * n, sizeof(double));
@@ -374,8 +414,15 @@ void oracle_jacob(int mech, double pres, const double* y, double* jac) {
         double dR_dT = e.Rf * e.dlnkf_dT - e.Rr * dlnkr;   /* at fixed C */
         double Sr = e.phi * (e.ordf * e.Rf - e.ordr * e.Rr);
         double thd_term = R * e.dphi_dthd;                  /* dq/dthd */
-        double dq_dT = e.phi * dR_dT + R * e.dphi_dT - (Sr + thd_term * e.thd) / T;
-        double s_r = Sr + thd_term * (e.thd - s.m);         /* sum_i dq/dC_i C_i */
+        double dq_dT, s_r;
+        if (!conv) {
+            dq_dT = e.phi * dR_dT + R * e.dphi_dT - (Sr + thd_term * e.thd) / T;
+            s_r = Sr + thd_term * (e.thd - s.m);            /* sum_i dq/dC_i C_i */
+        } else {
+            /* C fixed in T; P = m R T moves PLOG rates with T and with m */
+            dq_dT = e.phi * dR_dT + R * e.dphi_dT + q * e.dlnk_dlnP / T;
+            s_r = thd_term + q * e.dlnk_dlnP / s.m;         /* dq/dm, m = sum_i C_i */
+        }
         /* dq/dC_j for mass-action participants */
         double dqdC[2 * MAXP_ORACLE];
         int jsp[2 * MAXP_ORACLE], nj = 0;
@@ -414,41 +461,52 @@ void oracle_jacob(int mech, double pres, const double* y, double* jac) {
         }
     }
     const int N = n - 1;   /* closure species index */
-    double f[MAXNSP], dfdT[MAXNSP];
+    double f[MAXNSP], dfdT[MAXNSP], e[MAXNSP], c[MAXNSP];
+    /* energy per mass and heat capacity of each species: h, cp (constant
+       pressure) or u = h - R T / W_k, cv = cp - R / W_k (constant volume) */
+    for (int k = 0; k < n; ++k) {
+        e[k] = conv ? s.h[k] - RU * T / M->mw[k] : s.h[k];
+        c[k] = conv ? s.cp[k] - RU / M->mw[k] : s.cp[k];
+    }
+    const double c_avg = conv ? s.cp_avg - RU / s.mw_avg : s.cp_avg;
     /* species rows (including the closure row k = N) */
     double Q = 0.0;
     for (int k = 0; k < n; ++k) {
         f[k] = s.omega[k] * M->mw[k] / s.rho;
-        Q += s.h[k] * f[k];
-        dfdT[k] = (M->mw[k] / s.rho) * (domega_dT[k] + s.omega[k] / T);
+        Q += e[k] * f[k];
+        dfdT[k] = (M->mw[k] / s.rho) * (domega_dT[k] + (conv ? 0.0 : s.omega[k] / T));
     }
-    double fT = -Q / s.cp_avg;
+    double fT = -Q / c_avg;
     double* JY = (double*)calloc((size_t)n * n, sizeof(double));   /* JY[k*n + j], j < N */
     const double WN = M->mw[N];
     for (int k = 0; k < n; ++k) {
+        /* d/dY_j beyond the direct dC_j: rho(W) at constant pressure, m(C) at constant volume */
+        const double X = conv ? sk[k] : (s.mw_avg / s.rho) * (s.omega[k] - sk[k]);
         for (int j = 0; j < N; ++j) {
             double dj = 1.0 / M->mw[j] - 1.0 / WN;
-            JY[k * n + j] = M->mw[k] * (Jc[k * n + j] / M->mw[j] - Jc[k * n + N] / WN
-                                        + (s.mw_avg / s.rho) * dj * (s.omega[k] - sk[k]));
+            JY[k * n + j] = M->mw[k] * (Jc[k * n + j] / M->mw[j] - Jc[k * n + N] / WN + dj * X);
         }
     }
     /* assemble column-major output */
     for (int j = 0; j < N; ++j) {
         double acc = 0.0;
-        for (int k = 0; k < n; ++k) acc += s.h[k] * JY[k * n + j];
-        jac[0 + n * (j + 1)] = -(acc + fT * (s.cp[j] - s.cp[N])) / s.cp_avg;
+        for (int k = 0; k < n; ++k) acc += e[k] * JY[k * n + j];
+        jac[0 + n * (j + 1)] = -(acc + fT * (c[j] - c[N])) / c_avg;
         for (int k = 0; k < N; ++k) jac[(k + 1) + n * (j + 1)] = JY[k * n + j];
     }
     double accT = 0.0, dcp = 0.0;
     for (int k = 0; k < n; ++k) {
-        accT += s.cp[k] * f[k] + s.h[k] * dfdT[k];
+        accT += c[k] * f[k] + e[k] * dfdT[k];
         dcp += s.Y[k] * RU / M->mw[k] * dcp_R(nasa(M, k, T), T);
     }
-    jac[0] = -(accT + fT * dcp) / s.cp_avg;
+    jac[0] = -(accT + fT * dcp) / c_avg;
     for (int k = 0; k < N; ++k) jac[k + 1] = dfdT[k];
     free(Jc);
     free(JY);
 }
+
+void oracle_jacob(int mech, double pres, const double* y, double* jac) { jacob_impl(mech, pres, 0, y, jac); }
+void oracle_jacob_conv(int mech, double rho, const double* y, double* jac) { jacob_impl(mech, rho, 1, y, jac); }
 
 void oracle_gri30_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_GRI30, pres, y, dy); }
 void oracle_gri30_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_GRI30, pres, y, jac); }
@@ -460,3 +518,29 @@ void oracle_h2li_dydt(double t, double pres, const double* y, double* dy) { (voi
 void oracle_h2li_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_H2LI, pres, y, jac); }
 void oracle_estimate_dydt(double t, double pres, const double* y, double* dy) { (void)t; oracle_dydt(ORACLE_MECH_ESTIMATE, pres, y, dy); }
 void oracle_estimate_jacob(double t, double pres, const double* y, double* jac) { (void)t; oracle_jacob(ORACLE_MECH_ESTIMATE, pres, y, jac); }
+
+/* Constant-volume forms with pyJac's signature (the pres argument carries the
+ * cell's density), for the BDF driver. */
+#define CONV_FNS(tag, ID)                                                                              \
+    static void tag##_dydt_conv(double t, double rho, const double* y, double* dy) {                   \
+        (void)t; oracle_dydt_conv(ID, rho, y, dy);                                                       \
+    }                                                                                                    \
+    static void tag##_jacob_conv(double t, double rho, const double* y, double* jac) {                 \
+        (void)t; oracle_jacob_conv(ID, rho, y, jac);                                                     \
+    }
+CONV_FNS(gri30, ORACLE_MECH_GRI30)
+CONV_FNS(h2o2, ORACLE_MECH_H2O2)
+CONV_FNS(ndodecane, ORACLE_MECH_NDODECANE)
+CONV_FNS(h2li, ORACLE_MECH_H2LI)
+CONV_FNS(estimate, ORACLE_MECH_ESTIMATE)
+
+void oracle_mech_fns(int mech, int conv, oracle_rhs_fn* f, oracle_jac_fn* J) {
+    static const oracle_rhs_fn F[2][NMECH] = {
+        {oracle_gri30_dydt, oracle_h2o2_dydt, oracle_ndodecane_dydt, oracle_h2li_dydt, oracle_estimate_dydt},
+        {gri30_dydt_conv, h2o2_dydt_conv, ndodecane_dydt_conv, h2li_dydt_conv, estimate_dydt_conv}};
+    static const oracle_jac_fn G[2][NMECH] = {
+        {oracle_gri30_jacob, oracle_h2o2_jacob, oracle_ndodecane_jacob, oracle_h2li_jacob, oracle_estimate_jacob},
+        {gri30_jacob_conv, h2o2_jacob_conv, ndodecane_jacob_conv, h2li_jacob_conv, estimate_jacob_conv}};
+    *f = F[conv ? 1 : 0][mech];
+    *J = G[conv ? 1 : 0][mech];
+}

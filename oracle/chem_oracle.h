@@ -44,6 +44,17 @@ void oracle_estimate_jacob(double t, double pres, const double* y, double* jac);
 void oracle_dydt(int mech, double pres, const double* y, double* dy);
 void oracle_jacob(int mech, double pres, const double* y, double* jac);
 
+/* Constant-volume forms: rho is the cell's fixed density, the pressure
+ * follows from the state (P = rho R T / W); the energy equation conserves
+ * internal energy instead of enthalpy.  The reference's pyJac CONV branch
+ * (src/Mechanism/CPU/dydt.c:135-265, eval_conc_rho in chem_utils.c:99-137;
+ * it does not compile as shipped) states the same formulation. */
+void oracle_dydt_conv(int mech, double rho, const double* y, double* dy);
+void oracle_jacob_conv(int mech, double rho, const double* y, double* jac);
+void oracle_dydt_scale_conv(int mech, double rho, const double* y, double* scale);
+/* Density of the state y at pressure pres. */
+double oracle_density(int mech, double pres, const double* y);
+
 /* Forward rate coefficient of every reaction at (T, P), kf[nrxn] (falloff:
  * the high-pressure limit; PLOG: interpolated in ln P). */
 void oracle_kf(int mech, double pres, double T, double* kf);

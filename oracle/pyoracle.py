@@ -61,14 +61,19 @@ class Oracle:
         L = self.lib
         L.oracle_mech_nsp.restype = C.c_int
         L.oracle_mech_nsp.argtypes = [C.c_int]
-        for nm in ("oracle_dydt", "oracle_jacob", "oracle_dydt_scale"):
+        for nm in ("oracle_dydt", "oracle_jacob", "oracle_dydt_scale", "oracle_dydt_conv",
+                   "oracle_jacob_conv", "oracle_dydt_scale_conv"):
             getattr(L, nm).argtypes = [C.c_int, C.c_double, _dptr, _dptr]
             getattr(L, nm).restype = None
+        L.oracle_density.argtypes = [C.c_int, C.c_double, _dptr]
+        L.oracle_density.restype = C.c_double
         L.oracle_kf.argtypes = [C.c_int, C.c_double, C.c_double, _dptr]
         L.oracle_kf.restype = None
         L.oracle_bdf_batch_mech.restype = C.c_long
         L.oracle_bdf_batch_mech.argtypes = [C.c_int, C.c_long, _dptr, C.c_double, _dptr, C.c_double,
                                             C.c_double, C.POINTER(BdfOpts), C.c_void_p, C.c_int]
+        L.oracle_bdf_batch_mech_conv.restype = C.c_long
+        L.oracle_bdf_batch_mech_conv.argtypes = L.oracle_bdf_batch_mech.argtypes
         L.oracle_bdf_batch.restype = C.c_long
         L.oracle_bdf_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_long, _dptr, C.c_double,
                                        _dptr, C.c_double, C.c_double, C.POINTER(BdfOpts),
@@ -90,6 +95,30 @@ class Oracle:
         out = np.zeros_like(y)
         self.lib.oracle_dydt_scale(MECH_IDS[mech], float(pres), _p(y), _p(out))
         return out
+
+    # constant-volume forms: rho is the cell's fixed density
+    def dydt_conv(self, mech: str, rho: float, y: np.ndarray) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros_like(y)
+        self.lib.oracle_dydt_conv(MECH_IDS[mech], float(rho), _p(y), _p(out))
+        return out
+
+    def dydt_scale_conv(self, mech: str, rho: float, y: np.ndarray) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros_like(y)
+        self.lib.oracle_dydt_scale_conv(MECH_IDS[mech], float(rho), _p(y), _p(out))
+        return out
+
+    def jacob_conv(self, mech: str, rho: float, y: np.ndarray) -> np.ndarray:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        n = y.size
+        out = np.zeros(n * n)
+        self.lib.oracle_jacob_conv(MECH_IDS[mech], float(rho), _p(y), _p(out))
+        return out.reshape(n, n).T.copy()
+
+    def density(self, mech: str, pres: float, y: np.ndarray) -> float:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        return float(self.lib.oracle_density(MECH_IDS[mech], float(pres), _p(y)))
 
     def kf(self, mech: str, pres: float, T: float, nrxn: int) -> np.ndarray:
         """Forward rate coefficient of every reaction at (T, P)."""
@@ -125,8 +154,9 @@ class Oracle:
     # ------------------------------------------------------------------ BDF
     def bdf(self, mech: str, y: np.ndarray, pres, t1: float, rtol: float = 1e-6,
             atol: float = 1e-10, max_steps: int = 10000, threads: int = 1,
-            use_ref_kernels: bool = False, max_order: int = 5):
+            use_ref_kernels: bool = False, max_order: int = 5, conv: bool = False):
         """Integrate cell-major states y[ncells, n] from 0 to t1 in place-copy.
+        conv: constant volume (pres = each cell's initial pressure).
 
         Returns (y_out, stats structured array)."""
         y = np.array(y, dtype=np.float64, order="C", copy=True)
@@ -150,9 +180,9 @@ class Oracle:
             self.lib.oracle_bdf_batch(f, J, n, ncells, pp, pscal, _p(y), 0.0, float(t1),
                                       C.byref(opts), stats.ctypes.data_as(C.c_void_p), threads)
         else:
-            self.lib.oracle_bdf_batch_mech(MECH_IDS[mech], ncells, pp, pscal, _p(y), 0.0,
-                                           float(t1), C.byref(opts),
-                                           stats.ctypes.data_as(C.c_void_p), threads)
+            fn = self.lib.oracle_bdf_batch_mech_conv if conv else self.lib.oracle_bdf_batch_mech
+            fn(MECH_IDS[mech], ncells, pp, pscal, _p(y), 0.0, float(t1), C.byref(opts),
+               stats.ctypes.data_as(C.c_void_p), threads)
         return y, stats
 
 

@@ -50,6 +50,9 @@ def test_bad_b200_options_throw_before_device_work(driver):
     rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0,
                                   ["b200.max_steps=lots"])
     assert rc == 3 and "b200.max_steps: not an integer" in out
+    rc, out, *_ = host_driver.run(exe, d, "BDFIntegratorB200", "gri30.yaml", T, Y, 1e-6, 101325.0,
+                                  ["b200.formulation=isochoric"])
+    assert rc == 3 and "b200.formulation must be conp or conv" in out
 
 
 def test_no_device_is_a_runtime_error(driver):

@@ -55,14 +55,23 @@ def test_jacobian_TT_is_derivative_of_reference_rhs(oracle, golden_chem):
         assert abs(J[0, 0] - fd) <= 1e-5 * max(abs(fd), 1.0), (i, J[0, 0], fd)
 
 
+@pytest.mark.parametrize("conv", [False, True])
 @pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("gri30", "gri_32k"), ("nDodecane_Reitz", "nc12_8k"),
                                      ("ESTiMatE-Mech_04042022", "kero_2k")])
-def test_jacobian_finite_difference(oracle, mech, wl):
+def test_jacobian_finite_difference(oracle, mech, wl, conv):
+    """Analytic Jacobian against central differences of the RHS, at constant
+    pressure and at constant volume (density of the cell's state fixed)."""
     b = W.make(wl, 4, seed=7)
     ys = b.state_rows()
     for c in range(4):
         y = ys[c]
-        J = oracle.jacob(mech, b.P[c], y)
+        if conv:
+            rho = oracle.density(mech, b.P[c], y)
+            J = oracle.jacob_conv(mech, rho, y)
+            f = lambda v: oracle.dydt_conv(mech, rho, v)  # noqa: E731
+        else:
+            J = oracle.jacob(mech, b.P[c], y)
+            f = lambda v: oracle.dydt(mech, b.P[c], v)  # noqa: E731
         n = y.size
         Jfd = np.zeros((n, n))
         for j in range(n):
@@ -70,7 +79,7 @@ def test_jacobian_finite_difference(oracle, mech, wl):
             yp, ym = y.copy(), y.copy()
             yp[j] += h
             ym[j] -= h
-            Jfd[:, j] = (oracle.dydt(mech, b.P[c], yp) - oracle.dydt(mech, b.P[c], ym)) / (2 * h)
+            Jfd[:, j] = (f(yp) - f(ym)) / (2 * h)
         big = np.abs(Jfd) > 1e-4 * np.abs(Jfd).max()
         rel = np.abs(J - Jfd)[big] / np.abs(Jfd)[big]
         assert np.quantile(rel, 0.99) < 1e-3 and rel.max() < 1e-2, (c, rel.max())
@@ -160,3 +169,61 @@ def test_plog_rates_match_log_pressure_interpolation(oracle):
                     w = (lp - lnP[i]) / (lnP[i + 1] - lnP[i])
                     want = np.exp((1 - w) * np.log(level(i, T)) + w * np.log(level(i + 1, T)))
                 assert kf[r] == pytest.approx(want, rel=1e-12), (r, T, P)
+
+
+RU = 8314.4621
+
+
+def specific_energy(mech, T, Y, conv):
+    """Mixture enthalpy (constant pressure) or internal energy (constant
+    volume) per unit mass [J/kg] from the committed NASA-7 tables: T[n],
+    Y[nsp, n]."""
+    import os
+    import re
+    txt = open(os.path.join(W.MECH_DIR, f"{mech}_mech.h")).read()
+    t = {}
+    for m in re.finditer(r"static const double \w+?_(mw|tmid|nasa_lo|nasa_hi)\[\d+\] = \{([^}]*)\};", txt):
+        t[m.group(1)] = np.array([float(v) for v in m.group(2).split(",")])
+    n = t["mw"].size
+    T = np.atleast_1d(T)
+    lo, hi = t["nasa_lo"].reshape(n, 7), t["nasa_hi"].reshape(n, 7)
+    out = np.zeros(T.size)
+    for c in range(T.size):
+        a = np.where((T[c] <= t["tmid"])[:, None], lo, hi)
+        x = T[c]
+        hRT = a[:, 0] + x * (a[:, 1] / 2 + x * (a[:, 2] / 3 + x * (a[:, 3] / 4 + a[:, 4] / 5 * x))) + a[:, 5] / x
+        e = RU * x * hRT / t["mw"] - (RU * x / t["mw"] if conv else 0.0)
+        out[c] = (Y[:, c] * e).sum()
+    return out
+
+
+@pytest.mark.parametrize("conv", [False, True])
+def test_bdf_conserves_energy(oracle, conv):
+    """A closed adiabatic reactor conserves enthalpy at constant pressure and
+    internal energy at constant volume: after igniting H2 and CH4 cells at
+    rtol 1e-10 the change is round-off / tolerance level (< 1e-9 of cp T)."""
+    for wl in ("h2_1024", "gri_32k"):
+        b = W.make(wl, 4, seed=3)
+        ys = b.state_rows()
+        yo, st = oracle.bdf(b.mech, ys, b.P, b.dt, rtol=1e-10, atol=1e-14, conv=conv)
+        assert (st["status"] == 0).all()
+        full = lambda r: np.vstack([r[:, 1:].T, 1.0 - r[:, 1:].sum(axis=1)])  # noqa: E731
+        e0 = specific_energy(b.mech, ys[:, 0], full(ys), conv)
+        e1 = specific_energy(b.mech, yo[:, 0], full(yo), conv)
+        assert (yo[:, 0] - ys[:, 0]).max() > 500.0                      # they ignited
+        assert (np.abs(e1 - e0) / (1000.0 * yo[:, 0])).max() < 1e-9, (wl, conv)
+
+
+def test_constant_volume_raises_pressure(oracle):
+    """At constant volume the density stays that of the initial state and the
+    pressure P = rho R T / W rises with the heat release; at constant pressure
+    the density falls instead."""
+    b = W.make("h2_1024", 2, seed=3)
+    ys = b.state_rows()
+    rho0 = np.array([oracle.density(b.mech, b.P[c], ys[c]) for c in range(2)])
+    yv, _ = oracle.bdf(b.mech, ys, b.P, b.dt, rtol=1e-10, atol=1e-14, conv=True)
+    yp, _ = oracle.bdf(b.mech, ys, b.P, b.dt, rtol=1e-10, atol=1e-14)
+    for c in range(2):
+        rho_p = oracle.density(b.mech, b.P[c], yp[c])
+        P_v = b.P[c] * (rho0[c] / oracle.density(b.mech, b.P[c], yv[c]))   # P at rho0 and the final T, Y
+        assert rho_p < 0.7 * rho0[c] and P_v > 1.5 * b.P[c]
