@@ -107,3 +107,24 @@ def test_internal_energy_conserved_at_size():
     e1 = specific_energy(b.mech, T, Y, True)
     drift = np.abs(e1 - e0) / (1000.0 * T)
     assert drift.max() < 1e-5, drift.max()
+
+
+def test_persistent_equals_step_form():
+    """Both batching forms run the same step code at constant volume too."""
+    b = W.make("gri_32k", 64, seed=26)
+    out = []
+    for persistent in (1, 0):
+        s = native.Solver(b.mech, precision=native.B200ODE_FP64, persistent=persistent,
+                          formulation=native.B200ODE_CONV)
+        T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+        st, _, _ = s.integrate(T, Y, b.P, b.dt)
+        s.close()
+        out.append((T, Y, st))
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+def test_bad_formulation_is_refused():
+    with pytest.raises(native.B200Error) as e:
+        native.Solver("gri30", formulation=7)
+    assert e.value.code == 1 and "formulation" in str(e.value)

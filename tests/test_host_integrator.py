@@ -84,14 +84,18 @@ def test_quiescent_reference_case_through_cpp(driver, golden_e2e):
     ("gri_32k", "gri30.yaml", [], native.B200ODE_MIXED),
     ("h2_1024", "h2o2.yaml", [], native.B200ODE_MIXED),
     ("gri_32k", "gri30.yaml", ["b200.precision=fp64", "b200.form=step"], native.B200ODE_FP64),
-    ("h2li_grid", "h2_li_2004.xml", [], native.B200ODE_MIXED)])
+    ("h2li_grid", "h2_li_2004.xml", [], native.B200ODE_MIXED),
+    ("gri_32k", "gri30.yaml", ["b200.formulation=conv"], native.B200ODE_MIXED),
+    ("kero_2k", "ESTiMatE-Mech_04042022.xml", [], native.B200ODE_MIXED)])
 def test_reacting_cells_match_c_abi(driver, wl, mech, opts, precision):
     exe, d = driver
     b = W.make(wl, 48, seed=77)
     P = float(b.P[0])
     rc, out, To, Yo, st = host_driver.run(exe, d, "BDFIntegratorB200", mech, b.T, b.Y.T, b.dt, P, opts)
     assert rc == 0, out
-    s = native.Solver(b.mech, precision=precision)
+    conv = "b200.formulation=conv" in opts
+    s = native.Solver(b.mech, precision=precision,
+                      formulation=native.B200ODE_CONV if conv else native.B200ODE_CONP)
     T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
     st2, _, _ = s.integrate(T, Y, P, b.dt)
     s.close()
