@@ -250,17 +250,27 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         S.lu_dirty = 0;
         int status = 0;
         bool done = false;
+        bool ill = false;   // pressure not > 0 (or NaN): CVODE's CV_ILL_INPUT, cell left as given
         if (phase == 0) {
             Vec<MT::NS> y0;
             load_cell<MT>(p, cell, lane, y0.v);
-            S.P = pressure_slot<MT>(p, cell, y0.v, lane);
-            status = bdf_begin<MT, LinT>(off, y0, p.t0, p.t1, lane);
-            done = (status != 0);
+            const double P0 = p.P ? p.P[cell] : p.P_scalar;
+            if (!(P0 > 0.0)) {
+                ill = done = true;
+                status = cv::CV_ILL_INPUT;
+                for (int i = 0; i < 7; ++i) S.cnt[i] = 0;
+            } else {
+                S.P = pressure_slot<MT>(p, cell, y0.v, lane);
+                status = bdf_begin<MT, LinT>(off, y0, p.t0, p.t1, lane);
+                done = (status != 0);
+            }
         }
         if (!done) status = bdf_advance<MT, LinT>(off, wg, p.t1, p.steps, done, lane);
         if (done) {
-            const Vec<MT::NS> yo = bdf_finish<MT, LinT>(off, status, p.t1, lane);
-            store_cell<MT>(p, cell, lane, yo.v);
+            if (!ill) {
+                const Vec<MT::NS> yo = bdf_finish<MT, LinT>(off, status, p.t1, lane);
+                store_cell<MT>(p, cell, lane, yo.v);
+            }
             if (lane == 0) {
                 if (p.status) p.status[cell] = status;
                 for (int i = 0; i < 7; ++i)

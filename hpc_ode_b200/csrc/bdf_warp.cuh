@@ -50,7 +50,7 @@ enum { FIRST_CALL = 0, PREV_CONV_FAIL = 1, PREV_ERR_FAIL = 2 };
 enum { NO_FAILURES = 0, FAIL_BAD_J = 1, FAIL_OTHER = 2 };
 enum { DO_ERROR_TEST = 2, PREDICT_AGAIN = 3, TRY_AGAIN = 5, CONV_RECVR = 901 };
 enum { CV_SUCCESS = 0, CV_TOO_MUCH_WORK = -1, CV_TOO_MUCH_ACC = -2, CV_ERR_FAILURE = -3,
-       CV_CONV_FAILURE = -4, CV_TOO_CLOSE = -27 };
+       CV_CONV_FAILURE = -4, CV_ILL_INPUT = -22, CV_TOO_CLOSE = -27 };
 }  // namespace cv
 
 // Phases of the per-phase cycle profile.

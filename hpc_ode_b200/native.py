@@ -21,7 +21,7 @@ B200ODE_CONP = 0
 B200ODE_CONV = 1
 STATUS_NAMES = {0: "OK", 1: "ERR_INVALID", 2: "ERR_MECHANISM", 3: "ERR_CUDA", 4: "ERR_ALLOC",
                 5: "ERR_NO_DEVICE", 6: "ERR_BUSY", 7: "ERR_NOT_READY"}
-CELL_STATUS = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC",
+CELL_STATUS = {0: "CV_SUCCESS", -1: "CV_TOO_MUCH_WORK", -2: "CV_TOO_MUCH_ACC", -22: "CV_ILL_INPUT",
                -3: "CV_ERR_FAILURE", -4: "CV_CONV_FAILURE", -27: "CV_TOO_CLOSE"}
 
 # Every symbol include/b200ode.h declares.

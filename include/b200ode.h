@@ -52,6 +52,7 @@ enum {
     B200ODE_CELL_TOO_MUCH_ACC = -2,    /* CV_TOO_MUCH_ACC */
     B200ODE_CELL_ERR_FAILURE = -3,     /* CV_ERR_FAILURE: 7 error-test failures in one step */
     B200ODE_CELL_CONV_FAILURE = -4,    /* CV_CONV_FAILURE: 10 convergence failures in one step */
+    B200ODE_CELL_ILL_INPUT = -22,      /* CV_ILL_INPUT: the cell's pressure is not > 0 (cell left as given) */
     B200ODE_CELL_TOO_CLOSE = -27       /* CV_TOO_CLOSE: t1 too close to t0 */
 };
 

@@ -265,6 +265,28 @@ def test_poisoned_cells_do_not_disturb_neighbours(precision):
     assert st[7] != 0 and stats["n_failed"] >= 1
 
 
+@pytest.mark.parametrize("formulation", [native.B200ODE_CONP, native.B200ODE_CONV])
+def test_bad_pressure_is_ill_input(formulation):
+    """A per-cell pressure that is not > 0 (zero, negative, NaN) gives that cell
+    CVODE's CV_ILL_INPUT (-22) and leaves it as given; the other cells are
+    bitwise those of a clean run."""
+    b = W.make("gri_32k", 10, seed=12)
+    s = native.Solver("gri30", formulation=formulation)
+    Tc, Yc = b.T.copy(), b.Y.copy()
+    st_clean, _, _ = s.integrate(Tc, Yc, b.P, b.dt)
+    P = b.P.copy()
+    P[[1, 4, 8]] = [0.0, -101325.0, np.nan]
+    T, Y = b.T.copy(), b.Y.copy()
+    st, stats, cnt = s.integrate(T, Y, P, b.dt, counters=True)
+    s.close()
+    bad = np.array([1, 4, 8])
+    good = np.setdiff1d(np.arange(10), bad)
+    assert (st[bad] == -22).all() and stats["n_failed"] == 3 and (cnt["nst"][bad] == 0).all()
+    assert np.array_equal(T[bad], b.T[bad]) and np.array_equal(Y[:, bad], b.Y[:, bad])
+    assert np.array_equal(T[good], Tc[good]) and np.array_equal(Y[:, good], Yc[:, good])
+    assert np.array_equal(st[good], st_clean[good])
+
+
 def test_invalid_arguments_raise():
     with pytest.raises(native.B200Error):
         native.Solver("not_a_mechanism")
