@@ -69,15 +69,21 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
 
 enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3, MECH_ESTIMATE = 4 };
 
-#define MECH_TRAITS(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG>
-using GriT = MECH_TRAITS(MECH_GRI30, MECH_GRI30);
-using H2T = MECH_TRAITS(MECH_H2O2, MECH_H2O2);
-using NdT = MECH_TRAITS(MECH_NDODECANE_REITZ, MECH_NDODECANE);
-using H2LiT = MECH_TRAITS(MECH_H2_LI_2004, MECH_H2LI);
+// Traits of each compiled mechanism, per formulation (CV = 1: constant volume).
+#define MECH_TRAITS(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG, CV>
+template <int CV> using GriF = MECH_TRAITS(MECH_GRI30, MECH_GRI30);
+template <int CV> using H2F = MECH_TRAITS(MECH_H2O2, MECH_H2O2);
+template <int CV> using NdF = MECH_TRAITS(MECH_NDODECANE_REITZ, MECH_NDODECANE);
+template <int CV> using H2LiF = MECH_TRAITS(MECH_H2_LI_2004, MECH_H2LI);
 // kerosene (214 species): mixed precision only -- one warp's FP32 Newton
 // matrix (214 x 215 x 4 B = 184 KB) fills an SM's shared memory; the FP64
 // matrix would not fit
-using EstT = MECH_TRAITS(MECH_ESTIMATE_MECH_04042022, MECH_ESTIMATE);
+template <int CV> using EstF = MECH_TRAITS(MECH_ESTIMATE_MECH_04042022, MECH_ESTIMATE);
+using GriT = GriF<0>;
+using H2T = H2F<0>;
+using NdT = NdF<0>;
+using H2LiT = H2LiF<0>;
+using EstT = EstF<0>;
 static_assert(MECH_ESTIMATE + 1 == kNumMech, "one descriptor per mechanism");
 
 int mech_from_name(const char* name) {
@@ -124,7 +130,6 @@ struct KParams {
     double t0, t1, rtol, atol;
     int max_steps, max_order, refine, steps;
     int chunk;                        // persistent form: cells a warp claims per queue access
-    int conv;                         // constant volume: P is each cell's initial pressure
 };
 
 template <class MT>
@@ -140,9 +145,8 @@ __device__ __forceinline__ void load_cell(const KParams& p, long long cell, int 
 }
 
 // Density P W / (R T) of a cell's state at pressure P; y in internal order
-// [Y_0 .. Y_{N-2}, T].  In the constant-volume form the kernels carry -rho
-// in the pressure slot (the chemistry then takes rho as fixed, see
-// species_phase).
+// [Y_0 .. Y_{N-2}, T].  In the constant-volume form the kernels carry rho in
+// the pressure slot (the chemistry then takes it as fixed, see species_phase).
 template <class MT>
 __device__ __forceinline__ double cell_density(double P, const double (&y)[MT::NS], int lane) {
     constexpr int N = MT::N;
@@ -163,12 +167,13 @@ __device__ __forceinline__ double cell_density(double P, const double (&y)[MT::N
 }
 
 // The value the chemistry takes in its pressure slot: P (constant pressure) or
-// -rho of the state at P (constant volume).
+// the density of the state at P (constant volume: the density the cell keeps).
 template <class MT>
 __device__ __forceinline__ double pressure_slot(const KParams& p, long long cell, const double (&y)[MT::NS],
                                                 int lane) {
     const double P = p.P ? p.P[cell] : p.P_scalar;
-    return p.conv ? -cell_density<MT>(P, y, lane) : P;
+    if constexpr (MT::CONV) return cell_density<MT>(P, y, lane);
+    else return P;
 }
 
 template <class MT>
@@ -497,15 +502,22 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     return rc;
 }
 
-// Calls f(MT{}, LinT{}) with the handle's mechanism and Newton-matrix precision.
+template <int CV, class F>
+b200ode_status dispatch_form(const b200ode_handle* h, F&& f) {
+    const bool fp64 = h->opt.precision == B200ODE_FP64;
+    if (h->mech == MECH_GRI30) return fp64 ? f(GriF<CV>{}, double{}) : f(GriF<CV>{}, float{});
+    if (h->mech == MECH_NDODECANE) return fp64 ? f(NdF<CV>{}, double{}) : f(NdF<CV>{}, float{});
+    if (h->mech == MECH_H2LI) return fp64 ? f(H2LiF<CV>{}, double{}) : f(H2LiF<CV>{}, float{});
+    if (h->mech == MECH_ESTIMATE) return f(EstF<CV>{}, float{});   // FP64 refused at creation
+    return fp64 ? f(H2F<CV>{}, double{}) : f(H2F<CV>{}, float{});
+}
+
+// Calls f(MT{}, LinT{}) with the handle's mechanism, formulation and
+// Newton-matrix precision.
 template <class F>
 b200ode_status dispatch_mech(const b200ode_handle* h, F&& f) {
-    const bool fp64 = h->opt.precision == B200ODE_FP64;
-    if (h->mech == MECH_GRI30) return fp64 ? f(GriT{}, double{}) : f(GriT{}, float{});
-    if (h->mech == MECH_NDODECANE) return fp64 ? f(NdT{}, double{}) : f(NdT{}, float{});
-    if (h->mech == MECH_H2LI) return fp64 ? f(H2LiT{}, double{}) : f(H2LiT{}, float{});
-    if (h->mech == MECH_ESTIMATE) return f(EstT{}, float{});   // FP64 refused at creation
-    return fp64 ? f(H2T{}, double{}) : f(H2T{}, float{});
+    if (h->opt.formulation == B200ODE_CONV) return dispatch_form<1>(h, f);
+    return dispatch_form<0>(h, f);
 }
 
 b200ode_status run(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
@@ -601,7 +613,6 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
     p.max_order = h->opt.max_order;
     p.refine = h->opt.refine;
     p.chunk = std::max(1, std::min(h->opt.queue_chunk, 64));
-    p.conv = h->opt.formulation == B200ODE_CONV;
 }
 
 b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {

@@ -36,8 +36,11 @@ constexpr double kRU = 8314.4621;
 // count, descriptor index, the denominator of its stoichiometric coefficients
 // (1, or 2 / 4 with fractional product coefficients), its gather units and
 // whether it has PLOG reactions (the PLOG branch is compiled only then: the
-// reaction code is on the instruction-fetch-bound hot path).
-template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_>
+// reaction code is on the instruction-fetch-bound hot path), and the reactor
+// formulation: constant pressure, or constant volume (CONV_ = 1; the kernels'
+// pressure slot then carries the cell's fixed density).  Both are compile-time
+// so a kernel holds no code of the other case.
+template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_, int CONV_ = 0>
 struct MechT {
     static constexpr int ID = ID_;                            // index into c_mech
     static constexpr int N = N_;                              // state length == species count
@@ -48,6 +51,7 @@ struct MechT {
     static constexpr int NU_DEN = NU_DEN_;                    // gather words hold nu * NU_DEN
     static constexpr int NUNITMAX = NUNITS_;                  // gather units (checked at creation)
     static constexpr bool PLOG = NPLOG_ > 0;
+    static constexpr bool CONV = CONV_ != 0;
 };
 
 // Mechanism descriptors (one per compiled mechanism), set once per device.
@@ -180,14 +184,14 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     c.mw_avg = ode_div(1.0, warp_sum(sw));
     c.logT = log(c.T);
     c.invT = ode_div(1.0, c.T);
-    // P >= 0: constant pressure P.  P < 0: constant volume, -P is the cell's
-    // fixed density and the pressure follows from the state (P = rho R T / W).
-    if (P >= 0.0) {
+    if constexpr (!MT::CONV) {
         c.rho = ode_div(P * c.mw_avg, kRU * c.T);
         c.m = ode_div(P, kRU * c.T);
     } else {
-        c.rho = -P;
-        c.m = ode_div(-P, c.mw_avg);
+        // constant volume: P is the cell's fixed density, the pressure follows
+        // from the state (P = rho R T / W)
+        c.rho = P;
+        c.m = ode_div(P, c.mw_avg);
     }
     double csum = 0.0;
 #pragma unroll
@@ -467,15 +471,19 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
         for (int s = 0; s < MT::NS; ++s) om[s] = g.v[s];
     }
     // energy equation: enthalpy and cp at constant pressure; internal energy
-    // u = h - R T / W_k and cv = cp - R / W_k at constant volume (P < 0)
-    const double one = (P < 0.0) ? 1.0 : 0.0;
+    // u = h - R T / W_k and cv = cp - R / W_k at constant volume
     double qsum = 0.0, cpsum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
         const int i = lane + 32 * s;
         if (i < N) {
-            qsum += om[s] * (hRT[s] - one);
-            cpsum += (cpR[s] - one) * Yk[s] * __ldg(M.inv_mw + i);
+            if constexpr (!MT::CONV) {
+                qsum += om[s] * hRT[s];
+                cpsum += cpR[s] * Yk[s] * __ldg(M.inv_mw + i);
+            } else {
+                qsum += om[s] * (hRT[s] - 1.0);
+                cpsum += (cpR[s] - 1.0) * Yk[s] * __ldg(M.inv_mw + i);
+            }
         }
     }
     const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k e_k W_k   [W/m^3]
@@ -497,7 +505,7 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 // Analytic Jacobian J = d f / d y (internal order) into A (row-major, lda MT::LDA),
 // in precision LinT.  Chain rule through concentrations and the closure species:
 //   dC_i/dY_j = rho/W_i (delta_ij - delta_{i,N-1}) - C_i Wbar (1/W_j - 1/W_{N-1})
-// at constant pressure (rho = P Wbar / (R T)); at constant volume (P < 0, rho
+// at constant pressure (rho = P Wbar / (R T)); at constant volume (MT::CONV, rho
 // fixed) the second term is absent, C does not depend on T, and the total
 // concentration m = sum_i C_i (third bodies, PLOG pressure) adds
 // dw/dm (1/W_j - 1/W_{N-1}) rho to every column.
@@ -517,7 +525,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
 #pragma unroll 2
     for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
-    const bool conv = P < 0.0;   // constant volume (see species_phase)
+    constexpr bool conv = MT::CONV;   // constant volume (see species_phase)
     constexpr int ns = MT::NSLOT;
     const RxnCtx rc = rxn_ctx(c);
     const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
@@ -553,7 +561,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             for (int a = 0; a < 3; ++a) { ordf += (rf[a] < N); ordr += (pf[a] < N); }
             const double Sr = o.phi * (ordf * o.Rf - ordr * o.Rr);
             thd_term = R * o.dphi_dthd;
-            if (!conv) {
+            if constexpr (!conv) {
                 // C = rho Y / W with rho = P W / (R T): C and m fall as 1/T
                 dqdT = o.phi * dR_dT + R * o.dphi_dT - (Sr + thd_term * o.thd) * c.invT;
                 sr = Sr + thd_term * (o.thd - c.m);          // sum_i dq/dC_i C_i
@@ -634,11 +642,10 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             // constant pressure: energy h, heat capacity cp, f = w W / rho(T, Y);
             // constant volume: u = h - R T / W_k, cv = cp - R / W_k, rho fixed,
             // and sk holds dw/dm (m = sum_i C_i) instead of sum_i dw/dC_i C_i
-            const double one = conv ? 1.0 : 0.0;
-            dfdT[s] = Wr * (dw[s] + (conv ? 0.0 : w[s] * c.invT));
-            const double hW = RT * (hRT[s] - one);         // e_k W_k  [J/kmol]
-            const double hk = hW * iWi;                    // J/kg
-            const double cpk = kRU * (cpR[s] - one) * iWi; // J/kg/K
+            dfdT[s] = conv ? Wr * dw[s] : Wr * (dw[s] + w[s] * c.invT);
+            const double hW = conv ? RT * (hRT[s] - 1.0) : RT * hRT[s];                // e_k W_k  [J/kmol]
+            const double hk = hW * iWi;                                                 // J/kg
+            const double cpk = conv ? kRU * (cpR[s] - 1.0) * iWi : kRU * cpR[s] * iWi;  // J/kg/K
             const double X = conv ? sk[s] : (c.mw_avg * inv_rho) * (w[s] - sk[s]);
             spw[0 * N + i] = hW;
             spw[1 * N + i] = cpk;
