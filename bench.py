@@ -39,11 +39,11 @@ L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per cell of one k_bdf launch, from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum, 8,192-cell GRI capture, mixed precision): the traffic
 # is the compulsory T/P/Y in + T/Y/status out, so it scales with the cell count.
-NCU_DRAM_BYTES_PER_CELL = {"gri30": 842.0}
+NCU_DRAM_BYTES_PER_CELL = {"gri30": 789.0}
 # Warp instructions per cell of the same capture (smsp__inst_executed.sum / cells,
 # 8,192 GRI cells, mixed): the kernel is bound by instruction issue latency, so
 # issued instructions against the SMs' peak issue rate is its telling roofline.
-NCU_WARP_INSTR_PER_CELL = {("gri30", "mixed"): 3.314e6}
+NCU_WARP_INSTR_PER_CELL = {("gri30", "mixed"): 3.269e6}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 
 
@@ -403,7 +403,8 @@ def main():
                                    "k_bdf launch (profiles/k_bdf_gri8k_mixed_full.txt), scaled by cells"
                                    if per_cell else None),
                 "alg_bytes": alg_bytes,
-                "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
+                "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                                else "fallback 6,650 GB/s (MEASURED_PEAKS.json absent)"),
                 "note": "compute-bound path (FP64 CUDA-core pipe); HBM fraction shown for the "
                         "contract, see fp64 block and profiles/"}
     issue = None
