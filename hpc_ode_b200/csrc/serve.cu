@@ -150,6 +150,7 @@ std::string canonical_mech(const char* name) {
     if (!name) return std::string();
     std::string s(name);
     if (s.size() > 5 && s.substr(s.size() - 5) == ".yaml") s = s.substr(0, s.size() - 5);
+    else if (s.size() > 4 && s.substr(s.size() - 4) == ".xml") s = s.substr(0, s.size() - 4);
     return s;
 }
 
