@@ -189,15 +189,15 @@ def accuracy_block(batch: W.Batch, T_gpu: np.ndarray, Y_gpu: np.ndarray, nsample
 
 
 def serving_block(native, device: int, n_requests: int, load: float, seed: int = 4,
-                  chunk_cells: int = 32768) -> dict:
+                  chunk_cells: int = 32768, min_cells: int = 1024, max_cells: int = 262144) -> dict:
     """Serving loop under Poisson arrivals: requests of the serving workload
     (log-uniform 1k-256k cells, 60 % H2 / 40 % GRI, dt in {1e-5, 1e-4}) are
     submitted at exponential inter-arrival times with rate load x the measured
     saturation request rate; latency is submit -> results in the caller's host
     buffers (measured by the library's dispatcher thread).  Requests larger
     than chunk_cells run as consecutive launches of at most that many cells."""
-    cal = list(W.serving_requests(12, seed=seed + 1))
-    reqs = list(W.serving_requests(n_requests, seed=seed))
+    cal = list(W.serving_requests(12, seed=seed + 1, min_cells=min_cells, max_cells=max_cells))
+    reqs = list(W.serving_requests(n_requests, seed=seed, min_cells=min_cells, max_cells=max_cells))
     srv = native.Server(max_inflight=4, device=device, chunk_cells=chunk_cells)
     try:
         # saturation: the calibration requests submitted at once (also warms handles and staging)
@@ -233,8 +233,8 @@ def serving_block(native, device: int, n_requests: int, load: float, seed: int =
                 "cells_per_sec": cells / span, "cells": cells, "max_concurrent": rep["max_concurrent"],
                 "failed_cells": int(sum(i["n_failed"] for i in infos)),
                 "chunk_cells": chunk_cells,
-                "workload": "log-uniform 1k-256k cells, 60 % H2 (h2_1024 dists) / 40 % GRI (gri_32k dists), "
-                            "dt in {1e-5, 1e-4} s, Poisson arrivals, host buffers"}
+                "workload": f"log-uniform {min_cells}-{max_cells} cells, 60 % H2 (h2_1024 dists) / 40 % GRI "
+                            "(gri_32k dists), dt in {1e-5, 1e-4} s, Poisson arrivals, host buffers"}
     finally:
         srv.close()
 
