@@ -1023,6 +1023,14 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     rc = ensure_cap(h, (size_t)m);
     if (rc != B200ODE_OK) return rc;
     cudaStream_t st = h->stream;
+    // shared memory per warp, against a CTA's limit (shapes that exceed it are skipped)
+    size_t warp_smem = 0;
+    dispatch_mech(h, [&](auto mt, auto lt) {
+        warp_smem = warp_smem_bytes<decltype(mt), decltype(lt)>();
+        return B200ODE_OK;
+    });
+    int smem_optin = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
     // the sample: the first m cells, copied so the caller's buffers stay untouched
     double *sT = nullptr, *sY = nullptr;
     CUDA_TRY(cudaMallocAsync(&sT, m * sizeof(double), st));
@@ -1033,12 +1041,15 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     if (dP) CUDA_TRY(cudaMemcpyAsync(h->d_P, dP, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
     const b200ode_options saved = h->opt;
     // warps per CTA x register variant (blocks_per_sm >= 3 * 4 / wpb selects the
-    // 168-register variant, which trades spills for resident warps)
+    // 168-register variant, which trades spills for resident warps); shapes
+    // whose shared memory exceeds a CTA's (e.g. 4 or 2 warps of the 214-species
+    // mechanism) are skipped
     const int cand[6][2] = {{4, 0}, {2, 0}, {1, 0}, {4, 3}, {2, 6}, {1, 12}};
     float best_ms = 0.f;
     int best = -1;
     h->opt.persistent = 1;
     for (int c = 0; c < 6 && rc == B200ODE_OK; ++c) {
+        if ((size_t)cand[c][0] * warp_smem > (size_t)smem_optin) continue;
         h->opt.warps_per_block = cand[c][0];
         h->opt.blocks_per_sm = cand[c][1];
         float ms_c = 1e30f;
@@ -1070,6 +1081,7 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     cudaStreamSynchronize(st);
     h->opt = saved;
     if (rc != B200ODE_OK) return rc;
+    if (best < 0) return fail(B200ODE_ERR_CUDA, "autotune: no launch shape fits this device");
     h->opt.warps_per_block = cand[best][0];
     h->opt.blocks_per_sm = cand[best][1];
     if (wpb_out) *wpb_out = cand[best][0];

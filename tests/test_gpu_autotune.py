@@ -32,3 +32,28 @@ def test_autotune_picks_a_shape_and_results_do_not_change(precision):
     torch.cuda.synchronize()
     assert (st == 0).all()
     assert torch.equal(T, T2) and torch.equal(Y, Y2)
+
+
+def test_autotune_skips_shapes_that_do_not_fit():
+    """The 214-species mechanism fits one warp per CTA (its Newton matrix fills
+    the shared memory): the autotuner times only the shapes that fit and keeps
+    one of them."""
+    import torch
+    b = W.make("kero_2k", 148, seed=18)
+    T = torch.from_numpy(b.T.copy()).cuda()
+    Y = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
+    P = torch.from_numpy(b.P.copy()).cuda()
+    T0, Y0 = T.clone(), Y.clone()
+    s = native.Solver(b.mech)
+    wpb, bps = s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+    torch.cuda.synchronize()
+    assert wpb == 1 and bps in (0, 12)
+    assert torch.equal(T, T0) and torch.equal(Y, Y0)
+    s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+    s.close()
+    ref = native.Solver(b.mech)
+    T2, Y2 = T0.clone(), Y0.clone()
+    ref.integrate_device(b.ncells, P.data_ptr(), 0.0, T2.data_ptr(), Y2.data_ptr(), b.dt)
+    ref.close()
+    torch.cuda.synchronize()
+    assert torch.equal(T, T2) and torch.equal(Y, Y2)
