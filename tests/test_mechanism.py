@@ -101,3 +101,22 @@ def test_estimate_mechanism_forms():
     assert first.equation.startswith("CH3 + OH") and first.plog[0][0] == pytest.approx(0.01 * 101325.0)
     frac = [r for r in m.reactions if any(v != int(v) for _, v in r.prod)]
     assert len(frac) == 5 and not any(r.reversible for r in frac)
+
+
+def test_device_table_packing(tmp_path):
+    """The device-table packer (csrc/mech_dev.h, compiled with g++ here) accepts
+    every compiled mechanism; its gather-unit count equals the generated
+    NUNITS the kernels size their shared scratch by, its gather words
+    reproduce each net stoichiometric coefficient (fractional ones included),
+    and PLOG slots and inert species agree with the tables."""
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = tmp_path / "pack_check"
+    subprocess.run(["g++", "-O1", "-std=c++17", "-o", str(exe), os.path.join(here, "cpp", "pack_check.cpp")],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout
+    lines = out.stdout.strip().splitlines()
+    assert len(lines) == 5 and all(l.startswith("ok ") for l in lines)
+    est = [l for l in lines if "estimate" in l][0]
+    assert "plog 22" in est and "nu_den 2" in est
