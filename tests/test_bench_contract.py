@@ -1,0 +1,51 @@
+"""bench.py's one-line JSON contract: the keys, units and types a caller of the
+benchmark reads, for the reference arm (CPU only) and for a small run of the
+GPU arm."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(args, timeout=900):
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *args], cwd=ROOT,
+                         capture_output=True, text=True, timeout=timeout)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.strip().splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout
+    return json.loads(lines[0])
+
+
+def test_reference_arm_line():
+    d = _run(["--impl", "reference", "--steps", "1", "--warmup", "1", "--cpu-sample", "16"])
+    assert d["impl"] == "reference" and d["metric"] == "cells_per_sec" and d["unit"] == "cells/s"
+    assert d["value"] > 0 and d["higher_is_better"] is True and d["n_gpus"] == 1
+    assert d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["kind"] in ("reference", "port")
+    e = d["e2e"]
+    assert e["value"] == d["value"] and e["h2d_bytes_per_step"] == 0 and e["d2h_bytes_per_step"] == 0
+    assert d["config"]["workload"] == "gri_32k"
+
+
+@pytest.mark.gpu
+def test_gpu_arm_line():
+    d = _run(["--steps", "1", "--warmup", "3", "--ncells", "2048", "--no-serving", "--no-accuracy",
+              "--no-fp64-step", "--cpu-sample", "64"])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+              "scaling", "vs_baseline", "dtype", "data", "config", "roofline", "cpu_baseline", "e2e",
+              "clocks", "gpu_launches"):
+        assert k in d, k
+    assert d["metric"] == "cells_per_sec" and d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 3
+    assert d["scaling"] == "weak" and d["vs_baseline"] is None and d["gpu_launches"] >= 1
+    r = d["roofline"]
+    assert r["bound"] in ("hbm", "tensor") and r["unit"] in ("GB/s", "TFLOP/s")
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    e = d["e2e"]
+    assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert "sm_mhz" in d["clocks"] and "reasons" in d["clocks"]
+    assert d["cpu_baseline"]["value"] > 0 and d["failed_cells"] == 0
+    assert d["config"]["workload"] == "gri_32k" and d["config"]["cells_per_gpu"] == 2048
