@@ -130,6 +130,7 @@ struct KParams {
     double t0, t1, rtol, atol;
     int max_steps, max_order, refine, steps;
     int chunk;                        // persistent form: cells a warp claims per queue access
+    int helpers;                      // widest mechanisms: helper warps may serve warp 0
 };
 
 template <class MT>
@@ -206,15 +207,71 @@ __device__ __forceinline__ void store_cell(const KParams& p, long long cell, int
 // and give the same bits.
 // MINB: minimum resident 128-thread blocks per SM the register allocation must
 // allow (1 -> up to 255 registers, 3 -> at most 168); chosen by the autotuner.
+// Helper warp of a CTA that integrates one cell of a widest mechanism: runs the
+// shares warp 0 posts until it posts kCmdExit (or, bounded, stops posting).
+template <class MT, class LinT>
+__device__ __noinline__ void helper_loop(int wib, int lane) {
+    HelperCtl* h = &g_helper_ctl;
+    unsigned seen = 0;
+#pragma unroll 1
+    for (;;) {
+        const long long t0 = clock64();
+        unsigned cur;
+        bool idle_out = false;
+        while ((cur = ld_volatile(&h->seq)) == seen) {
+            if (clock64() - t0 > kHelperIdleCycles) { idle_out = true; break; }
+            __nanosleep(32);
+        }
+        __syncwarp();
+        if (__any_sync(kFull, idle_out)) {
+            if (lane == 0) h->err = 1;
+            return;
+        }
+        __threadfence_block();
+        seen = cur;
+        const int cmd = *(const volatile int*)&h->cmd;
+        if (cmd == kCmdExit) return;
+        if (cmd == kCmdRhs)
+            rhs_groups<MT>(h->rc, h->C_off, h->G_off, h->q_off, wib, kHelperWarps + 1, lane);
+        else if (cmd == kCmdLu)
+            lu_trailing<MT, LinT>(smem_at<LinT>(h->A_off), h->k0, h->kend, lane, wib, kHelperWarps + 1);
+        __threadfence_block();
+        __syncwarp();
+        if (lane == 0) atomicAdd(&h->done, 1u);
+    }
+}
+
 template <class MT, class LinT, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KParams p) {
     using R = StepRecord<MT, LinT>;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
+    long long cells_per_block = blockDim.x >> 5;
+    if constexpr (MT::N >= kWideN) {
+        // one cell per CTA: warp 0 integrates, warps 1-3 serve it (see HelperCtl)
+        HelperCtl* hc = &g_helper_ctl;
+        const bool serve = p.helpers && blockDim.x == 32 * (kHelperWarps + 1);
+        if (threadIdx.x == 0) {
+            hc->seq = 0;
+            hc->done = 0;
+            hc->posted = 0;
+            hc->cmd = 0;
+            hc->err = 0;
+            hc->nhelpers = serve ? kHelperWarps : 0;
+        }
+        __syncthreads();
+        if (serve) {
+            if (wib != 0) {
+                helper_loop<MT, LinT>(wib, lane);
+                return;
+            }
+            cells_per_block = 1;
+        }
+    }
     auto* w = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     const unsigned off = smem_off(w);
     BdfState& S = w->st;
-    const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    const long long gw = (long long)blockIdx.x * cells_per_block + wib;
     const bool step_form = p.records != nullptr;
     auto* wglob = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal);
     const int profiling = (p.prof != nullptr && !step_form) ? 1 : 0;
@@ -256,6 +313,8 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         int status = 0;
         bool done = false;
         bool ill = false;   // pressure not > 0 (or NaN): CVODE's CV_ILL_INPUT, cell left as given
+        int helper_err0 = 0;
+        if constexpr (MT::N >= kWideN) helper_err0 = g_helper_ctl.err;
         if (phase == 0) {
             Vec<MT::NS> y0;
             load_cell<MT>(p, cell, lane, y0.v);
@@ -271,6 +330,13 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
             }
         }
         if (!done) status = bdf_advance<MT, LinT>(off, wg, p.t1, p.steps, done, lane);
+        if constexpr (MT::N >= kWideN) {
+            // a helper wait ran out during this cell: its factors may be incomplete
+            if (g_helper_ctl.err != helper_err0 && status == 0) {
+                status = cv::CV_ERR_FAILURE;
+                done = true;
+            }
+        }
         if (done) {
             if (!ill) {
                 const Vec<MT::NS> yo = bdf_finish<MT, LinT>(off, status, p.t1, lane);
@@ -286,6 +352,9 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
             tot[7] += (status != 0);
         }
         if (step_form) bdf_save<MT, LinT>(off, rec, done ? 2 : 1, lane);
+    }
+    if constexpr (MT::N >= kWideN) {
+        if (g_helper_ctl.nhelpers == kHelperWarps) helpers_post(&g_helper_ctl, kCmdExit, lane);
     }
     if (lane == 0)
         for (int i = 0; i < 8; ++i)
@@ -303,6 +372,10 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParams p, double* dTdt, double* dYdt) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if constexpr (MT::N >= kWideN) {   // no helper warps here
+        if (threadIdx.x == 0) g_helper_ctl.nhelpers = 0;
+        __syncthreads();
+    }
     const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (cell >= p.ncells) return;
     auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
@@ -322,6 +395,10 @@ __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParam
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParams p, double* jac) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    if constexpr (MT::N >= kWideN) {   // no helper warps here
+        if (threadIdx.x == 0) g_helper_ctl.nhelpers = 0;
+        __syncthreads();
+    }
     const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
     if (cell >= p.ncells) return;
     auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
@@ -422,6 +499,14 @@ int pick_wpb(b200ode_handle* h) {
     return best;
 }
 
+// Threads per CTA of the BDF kernel for wpb cells per CTA: one 128-thread CTA
+// per cell when a widest mechanism's helper warps serve (wpb = 1).
+template <class MT>
+int bdf_threads(const b200ode_handle* h, int wpb) {
+    if (MT::N >= kWideN && wpb == 1 && h->opt.cta_helpers) return 32 * (kHelperWarps + 1);
+    return wpb * 32;
+}
+
 template <class MT, class LinT>
 b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* launches) {
     using R = StepRecord<MT, LinT>;
@@ -437,7 +522,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     p.done_count = h->d_ctl + 9;
     if (h->opt.persistent) {
         int bps = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, wpb * 32, smem));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, bdf_threads<MT>(h, wpb), smem));
         if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
         if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
         h->last_blocks_per_sm = bps;
@@ -448,7 +533,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
         p.wglobal = h->d_wg;
         p.records = nullptr;
         p.steps = 0x7fffffff;
-        kern<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+        kern<<<(unsigned)blocks, bdf_threads<MT>(h, wpb), smem, st>>>(p);
         CUDA_TRY(cudaGetLastError());
         *launches += 1;
         return B200ODE_OK;
@@ -475,7 +560,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     if (h->opt.use_graph) {
         cudaGraph_t g;
         CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < per_check; ++i) kern<<<blocks, wpb * 32, smem, st>>>(p);
+        for (int i = 0; i < per_check; ++i) kern<<<blocks, bdf_threads<MT>(h, wpb), smem, st>>>(p);
         CUDA_TRY(cudaStreamEndCapture(st, &g));
         cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
         cudaGraphDestroy(g);
@@ -488,7 +573,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
         if (gexec) {
             if (cudaGraphLaunch(gexec, st) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "cudaGraphLaunch"); break; }
         } else {
-            kern<<<blocks, wpb * 32, smem, st>>>(p);
+            kern<<<blocks, bdf_threads<MT>(h, wpb), smem, st>>>(p);
         }
         *launches += per_check;
         if (cudaMemcpyAsync(h->h_done, p.done_count, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -536,7 +621,7 @@ b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KP
     if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) k = k_bdf<MT, LinT, 3>;
     CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int bps = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, wpb * 32, smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, bdf_threads<MT>(h, wpb), smem));
     if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
     if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
     long long b = (long long)bps * h->num_sms;
@@ -613,6 +698,7 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
     p.max_order = h->opt.max_order;
     p.refine = h->opt.refine;
     p.chunk = std::max(1, std::min(h->opt.queue_chunk, 64));
+    p.helpers = h->opt.cta_helpers != 0;
 }
 
 b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {
@@ -672,7 +758,7 @@ b200ode_status launch_persistent(b200ode_handle* h, int64_t n, const double* dP,
         b200ode_status rc = persistent_shape<MT, LinT>(h, n, &k, &blocks, &wpb, &smem);
         if (rc != B200ODE_OK) return rc;
         CUDA_TRY(cudaMemsetAsync(ctl, 0, kCtlWords * sizeof(unsigned long long), st));
-        k<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+        k<<<(unsigned)blocks, bdf_threads<MT>(h, wpb), smem, st>>>(p);
         CUDA_TRY(cudaGetLastError());
         return B200ODE_OK;
     });
@@ -699,6 +785,7 @@ void b200ode_default_options(b200ode_options* o) {
     o->device = -1;
     o->profile_phases = 0;
     o->formulation = B200ODE_CONP;
+    o->cta_helpers = 1;
 }
 
 const char* b200ode_last_error(void) { return g_last_error.c_str(); }

@@ -407,6 +407,110 @@ __device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, u
 
 __device__ __forceinline__ RxnCtx rxn_ctx(const CellThermo& c) { return RxnCtx{c.T, c.logT, c.invT, c.m, c.mC}; }
 
+// ---- One cell on a CTA's four warps (mechanisms of kWideN+ unknowns).
+// Their Newton matrix fills an SM's shared memory, so one cell runs per SM and
+// a single warp would leave three of the SM's four schedulers idle.  Warp 0
+// runs the integration; warps 1-3 ("helpers") take a share of its two widest
+// loops -- the reaction groups of the RHS and the trailing update of the
+// blocked LU -- when warp 0 posts them.  Each share writes disjoint outputs
+// with the same operations a single warp would use, so results do not depend
+// on whether helpers serve.  The hand-off goes through a shared-memory control
+// block with bounded polling waits (no hardware barrier a warp could miss).
+constexpr int kWideN = 192;
+constexpr int kHelperWarps = 3;
+enum { kCmdRhs = 1, kCmdLu = 2, kCmdExit = 3 };
+// A helper waits for the next command at most ~10 s (warp 0 works alone
+// between commands: Jacobian, step control); warp 0 waits for a command's
+// completion at most ~2 s (a share takes microseconds).
+constexpr long long kHelperIdleCycles = 20000000000LL;
+constexpr long long kJoinCycles = 4000000000LL;
+
+struct HelperCtl {
+    unsigned seq;      // commands posted
+    unsigned done;     // helper completions (kHelperWarps per command)
+    unsigned posted;   // warp 0's count of commands posted
+    int cmd;
+    int nhelpers;      // kHelperWarps while the helpers serve, else 0
+    int err;           // a bounded wait ran out
+    int k0, kend;      // kCmdLu: the LU panel
+    unsigned A_off, C_off, G_off, q_off;
+    RxnCtx rc;         // kCmdRhs: the cell's reaction context
+};
+// One per CTA, in the kernels of the mechanisms that use it.
+__shared__ HelperCtl g_helper_ctl;
+
+__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
+
+// Warp 0: post a command whose arguments it has written (every lane's earlier
+// shared-memory writes are made visible to the helpers first).
+__device__ __forceinline__ void helpers_post(HelperCtl* h, int cmd, int lane) {
+    __threadfence_block();
+    __syncwarp();
+    if (lane == 0) {
+        h->cmd = cmd;
+        h->posted += 1;
+        __threadfence_block();
+        atomicAdd(&h->seq, 1u);
+    }
+    __syncwarp();
+}
+
+// Warp 0: wait until the helpers have finished every posted command.  If the
+// wait runs out, the helpers are dropped (nhelpers = 0) and err is set.
+__device__ __forceinline__ void helpers_join(HelperCtl* h, int lane) {
+    const unsigned expected = kHelperWarps * h->posted;
+    const long long t0 = clock64();
+    bool ok = true;
+    while (ld_volatile(&h->done) < expected) {
+        if (clock64() - t0 > kJoinCycles) { ok = false; break; }
+    }
+    __threadfence_block();
+    ok = __all_sync(kFull, ok);
+    if (!ok && lane == 0) {
+        h->err = 1;
+        h->nhelpers = 0;
+    }
+    __syncwarp();
+}
+
+// Rates of progress of the reaction groups g = g0, g0 + dg, ... into the
+// shared rate array at byte offset q_off.
+template <class MT>
+__device__ __forceinline__ void rhs_groups(const RxnCtx rc, unsigned C_off, unsigned G_off, unsigned q_off, int g0,
+                                           int dg, int lane) {
+    double* q = smem_at<double>(q_off);
+#pragma unroll 1
+    for (int g = g0; g < MT::NG; g += dg) {
+        const int s = 32 * g + lane;
+        q[s] = rxn_slot<MT>(s, rc, C_off, G_off, 0).q;
+    }
+}
+
+// The RHS's reaction groups on warp 0, with the CTA's helper warps taking every
+// (kHelperWarps + 1)-th group from their own index when they serve it.
+template <class MT>
+__device__ __forceinline__ void rhs_groups_forked(const RxnCtx rc, unsigned C_off, unsigned G_off, unsigned q_off,
+                                                  int lane) {
+    HelperCtl* h = &g_helper_ctl;
+    if (h->nhelpers != kHelperWarps) {
+        rhs_groups<MT>(rc, C_off, G_off, q_off, 0, 1, lane);
+        return;
+    }
+    if (lane == 0) {
+        h->rc = rc;
+        h->C_off = C_off;
+        h->G_off = G_off;
+        h->q_off = q_off;
+    }
+    helpers_post(h, kCmdRhs, lane);
+    constexpr int dg = kHelperWarps + 1;
+    rhs_groups<MT>(rc, C_off, G_off, q_off, 0, dg, lane);
+    helpers_join(h, lane);
+    if (h->err) {   // helpers dropped: their groups again on this warp (the same values)
+        for (int w = 1; w < dg; ++w) rhs_groups<MT>(rc, C_off, G_off, q_off, w, dg, lane);
+    }
+}
+
 // Balanced gather: out[s] = sum over species (lane + 32 s)'s (slot, nu) pairs of
 // nu * src[slot]; src is the shared-memory array at byte offset src_off, or,
 // with kGlobal, the global array gsrc.  Unit partial sums go through the
@@ -458,10 +562,14 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
     const RxnCtx rc = rxn_ctx(c);
     const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
+    if constexpr (MT::N >= kWideN) {
+        rhs_groups_forked<MT>(rc, C_off, G_off, smem_off(sm->q), lane);
+    } else {
 #pragma unroll 1
-    for (int g = 0; g < MT::NG; ++g) {
-        const int s = 32 * g + lane;
-        sm->q[s] = rxn_slot<MT>(s, rc, C_off, G_off, 0).q;
+        for (int g = 0; g < MT::NG; ++g) {
+            const int s = 32 * g + lane;
+            sm->q[s] = rxn_slot<MT>(s, rc, C_off, G_off, 0).q;
+        }
     }
     __syncwarp();
     double om[MT::NS];

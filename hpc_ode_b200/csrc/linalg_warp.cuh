@@ -24,6 +24,86 @@ namespace b200 {
 template <class T>
 __device__ __forceinline__ T absT(T v) { return v < T(0) ? -v : v; }
 
+// Trailing update A22 -= L21 U12 of the blocked LU after panel [k0, kend) for
+// the columns j = lane + 32 s of the slots s with s % nw == w (nw warps share
+// the columns; nw = 1: all).  The block rows' entries u are read from A (row
+// k0 as the panel left it, rows k0+1.. as U12 stored them); rows go in batches
+// of kRows whose multipliers and entries are loaded before any store.  Each
+// element receives the same fused multiply-adds in the same order whichever
+// warp updates it, so splitting the columns does not change the factors.
+template <class MT, class LinT>
+__device__ __forceinline__ void lu_trailing(LinT* A, int k0, int kend, int lane, int w, int nw) {
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    constexpr int kPanel = 4;
+    constexpr int kRows = sizeof(LinT) == 4 ? 8 : 4;
+    LinT u[kPanel][NS];
+    bool on[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int j = lane + 32 * s;
+        const bool mine = j >= kend && j < N && (s % nw) == w;
+        bool nz = false;
+#pragma unroll
+        for (int r = 0; r < kPanel; ++r) {
+            u[r][s] = (mine && k0 + r < kend) ? A[(k0 + r) * LDA + j] : LinT(0);
+            nz = nz || (u[r][s] != LinT(0));
+        }
+        on[s] = mine && nz;   // columns with a zero U12 block need no update
+    }
+#pragma unroll 1
+    for (int i0 = kend; i0 < N; i0 += kRows) {
+        const int nr = min(kRows, N - i0);
+        LinT l[kRows][kPanel];
+#pragma unroll
+        for (int rr = 0; rr < kRows; ++rr)
+#pragma unroll
+            for (int q = 0; q < kPanel; ++q)
+                l[rr][q] = (rr < nr && k0 + q < kend) ? A[(i0 + rr) * LDA + k0 + q] : LinT(0);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            if (on[s]) {
+                const int j = lane + 32 * s;
+                LinT a[kRows];
+#pragma unroll
+                for (int rr = 0; rr < kRows; ++rr)
+                    if (rr < nr) a[rr] = A[(i0 + rr) * LDA + j];
+#pragma unroll
+                for (int q = 0; q < kPanel; ++q) {
+                    if (u[q][s] != LinT(0)) {
+#pragma unroll
+                        for (int rr = 0; rr < kRows; ++rr) a[rr] = a[rr] - l[rr][q] * u[q][s];
+                    }
+                }
+#pragma unroll
+                for (int rr = 0; rr < kRows; ++rr)
+                    if (rr < nr) A[(i0 + rr) * LDA + j] = a[rr];
+            }
+        }
+    }
+}
+
+// The trailing update run by warp 0, with the CTA's helper warps taking their
+// share of the columns when they serve it (mechanisms of kWideN+ unknowns).
+template <class MT, class LinT>
+__device__ __forceinline__ void lu_trailing_forked(unsigned A_off, int k0, int kend, int lane) {
+    LinT* A = smem_at<LinT>(A_off);
+    if constexpr (MT::N >= kWideN) {
+        HelperCtl* h = &g_helper_ctl;
+        if (h->nhelpers == kHelperWarps) {
+            if (lane == 0) {
+                h->A_off = A_off;
+                h->k0 = k0;
+                h->kend = kend;
+            }
+            helpers_post(h, kCmdLu, lane);
+            lu_trailing<MT, LinT>(A, k0, kend, lane, 0, kHelperWarps + 1);
+            helpers_join(h, lane);
+            return;
+        }
+    }
+    lu_trailing<MT, LinT>(A, k0, kend, lane, 0, 1);
+}
+
 // LU factorization in place (both forms below give the same factors).  perm =
 // the composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
 // Returns 0, or k+1 if U_kk == 0 (singular).  All 32 lanes call it.
@@ -149,43 +229,11 @@ __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off
                 for (int r = 1; r < kPanel; ++r)
                     if (k0 + r < kend) A[(k0 + r) * LDA + j] = u[r][s];
             }
-            bool nz = false;
-#pragma unroll
-            for (int r = 0; r < kPanel; ++r) nz = nz || (u[r][s] != LinT(0));
-            on[s] = on[s] && nz;   // columns with a zero U12 block need no update
         }
         __syncwarp();
-        // ---- 3. trailing update A22 -= L21 U12, rows in batches of kRows
-#pragma unroll 1
-        for (int i0 = kend; i0 < N; i0 += kRows) {
-            const int nr = min(kRows, N - i0);
-            LinT l[kRows][kPanel];
-#pragma unroll
-            for (int rr = 0; rr < kRows; ++rr)
-#pragma unroll
-                for (int q = 0; q < kPanel; ++q)
-                    l[rr][q] = (rr < nr && k0 + q < kend) ? A[(i0 + rr) * LDA + k0 + q] : LinT(0);
-#pragma unroll
-            for (int s = 0; s < NS; ++s) {
-                if (on[s]) {
-                    const int j = lane + 32 * s;
-                    LinT a[kRows];
-#pragma unroll
-                    for (int rr = 0; rr < kRows; ++rr)
-                        if (rr < nr) a[rr] = A[(i0 + rr) * LDA + j];
-#pragma unroll
-                    for (int q = 0; q < kPanel; ++q) {
-                        if (u[q][s] != LinT(0)) {
-#pragma unroll
-                            for (int rr = 0; rr < kRows; ++rr) a[rr] = a[rr] - l[rr][q] * u[q][s];
-                        }
-                    }
-#pragma unroll
-                    for (int rr = 0; rr < kRows; ++rr)
-                        if (rr < nr) A[(i0 + rr) * LDA + j] = a[rr];
-                }
-            }
-        }
+        // ---- 3. trailing update A22 -= L21 U12 (split over the CTA's helper warps
+        // when they serve this warp, see lu_trailing)
+        lu_trailing_forked<MT, LinT>(A_off, k0, kend, lane);
         __syncwarp();
     }
 #pragma unroll

@@ -52,7 +52,7 @@ class Options(C.Structure):
                 ("persistent", C.c_int32), ("warps_per_block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("queue_chunk", C.c_int32),
                 ("use_graph", C.c_int32), ("device", C.c_int32), ("profile_phases", C.c_int32),
-                ("formulation", C.c_int32)]
+                ("formulation", C.c_int32), ("cta_helpers", C.c_int32)]
 
 
 _i32p = C.POINTER(C.c_int32)

@@ -84,6 +84,10 @@ typedef struct {
     int32_t device;           /* CUDA device ordinal (-1 = current) */
     int32_t profile_phases;   /* 1 = accumulate per-phase device cycles into b200ode_stats */
     int32_t formulation;      /* B200ODE_CONP (default) or B200ODE_CONV */
+    int32_t cta_helpers;      /* mechanisms whose Newton matrix fills an SM (one cell per SM):
+                                 1 (default) = the CTA's other three warps take shares of the
+                                 cell's reaction groups and LU updates; 0 = one warp per cell.
+                                 Results are the same either way. */
 } b200ode_options;
 
 /* Optional per-cell counters (CVodeGetNum* equivalents) and call totals.  Any

@@ -110,3 +110,22 @@ def test_persistent_equals_step_form():
         out.append((T, Y, st))
     assert np.array_equal(out[0][2], out[1][2])
     assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_helper_warps_do_not_change_results(persistent):
+    """One cell per SM: by default the CTA's other three warps take shares of
+    warp 0's reaction groups and LU updates.  Each share writes disjoint
+    outputs with the operations a single warp uses, so the results, statuses
+    and step counts equal those of the one-warp launch bitwise."""
+    b = _cells(24, seed=9)
+    out = []
+    for helpers in (1, 0):
+        s = native.Solver(MECH, persistent=persistent, cta_helpers=helpers)
+        T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+        st, stats, cnt = s.integrate(T, Y, b.P, b.dt, counters=True)
+        s.close()
+        out.append((T, Y, st, cnt["nst"]))
+    assert (out[0][2] == 0).all()
+    for a, c in zip(out[0], out[1]):
+        assert np.array_equal(a, c)
