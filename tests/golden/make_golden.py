@@ -1,7 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference.
 
-Run in a checkout that has the reference tree (REF_DIR, default the read-only
-reference mount) and its pyJac C built by ``make -C oracle ref``:
+Run in a checkout that has the reference tree (REF_DIR; default HPC_ODE_REFERENCE,
+else BASELINE.json's reference_path) and its pyJac C built by ``make -C oracle ref``:
 
     python tests/golden/make_golden.py [REF_DIR]
 
@@ -86,7 +86,10 @@ def enthalpy_fixture(ref_dir: str):
 
 if __name__ == "__main__":
     args = [a for a in sys.argv[1:] if not a.startswith("--") and a != "enthalpy"]
-    ref = args[0] if args else "/root/reference"
+    from oracle.refpath import reference_dir
+    ref = args[0] if args else reference_dir()
+    if not ref:
+        raise SystemExit("no reference checkout: pass REF_DIR or set HPC_ODE_REFERENCE")
     if "--only" in sys.argv and sys.argv[sys.argv.index("--only") + 1] == "enthalpy":
         enthalpy_fixture(ref)
     else:

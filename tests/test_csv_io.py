@@ -8,8 +8,9 @@ import numpy as np
 import pytest
 
 from hpc_ode_b200 import build, io
+from oracle.refpath import reference_subdir
 
-REF_DATA = "/root/reference/ref_data"
+REF_DATA = reference_subdir("ref_data") or ""
 
 
 @pytest.fixture(scope="module", autouse=True)

@@ -12,8 +12,10 @@ import pytest
 from hpc_ode_b200 import mechanism as M
 from hpc_ode_b200 import workloads as W
 
-REF_MECH = "/root/reference/resources/mechanisms"
-REF_DATA = "/root/reference/ref_data"
+from oracle.refpath import reference_subdir  # noqa: E402
+
+REF_MECH = reference_subdir("resources", "mechanisms") or ""
+REF_DATA = reference_subdir("ref_data") or ""
 needs_ref = pytest.mark.skipif(not os.path.isdir(REF_MECH), reason="reference mechanisms not present")
 
 
