@@ -69,12 +69,14 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
 
 enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3, MECH_ESTIMATE = 4 };
 
-// Traits of each compiled mechanism, per formulation (CV = 1: constant volume).
+// Traits of each compiled mechanism, per formulation (CV = 1: constant
+// volume) and, for the two H2 mechanisms (9-10 unknowns), lanes per cell.
 #define MECH_TRAITS(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG, CV>
+#define MECH_TRAITS_G(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG, CV, G>
 template <int CV> using GriF = MECH_TRAITS(MECH_GRI30, MECH_GRI30);
-template <int CV> using H2F = MECH_TRAITS(MECH_H2O2, MECH_H2O2);
+template <int CV, int G = 32> using H2F = MECH_TRAITS_G(MECH_H2O2, MECH_H2O2);
 template <int CV> using NdF = MECH_TRAITS(MECH_NDODECANE_REITZ, MECH_NDODECANE);
-template <int CV> using H2LiF = MECH_TRAITS(MECH_H2_LI_2004, MECH_H2LI);
+template <int CV, int G = 32> using H2LiF = MECH_TRAITS_G(MECH_H2_LI_2004, MECH_H2LI);
 // kerosene (214 species): mixed precision only -- one warp's FP32 Newton
 // matrix (214 x 215 x 4 B = 184 KB) fills an SM's shared memory; the FP64
 // matrix would not fit
@@ -85,6 +87,9 @@ using NdT = NdF<0>;
 using H2LiT = H2LiF<0>;
 using EstT = EstF<0>;
 static_assert(MECH_ESTIMATE + 1 == kNumMech, "one descriptor per mechanism");
+
+// Lanes per cell the H2 mechanisms use unless the options say otherwise.
+constexpr int kSmallMechLanes = 16;
 
 int mech_from_name(const char* name) {
     if (!name) return -1;
@@ -115,6 +120,7 @@ int dispatch_units(int mech) {
 // ---------------------------------------------------------------- kernels
 struct KParams {
     long long ncells;
+    long long pitch;                  // row stride of Y in cells (>= ncells; a chunk of a larger batch)
     const double* P;
     double P_scalar;
     double* T;
@@ -131,6 +137,9 @@ struct KParams {
     int max_steps, max_order, refine, steps;
     int chunk;                        // persistent form: cells a warp claims per queue access
     int helpers;                      // widest mechanisms: helper warps may serve warp 0
+    long long helper_join_cycles;     // helper hand-off wait limits (0 = defaults, see HelperCtl)
+    long long helper_drain_cycles;
+    long long helper_idle_cycles;
 };
 
 template <class MT>
@@ -138,8 +147,8 @@ __device__ __forceinline__ void load_cell(const KParams& p, long long cell, int 
     constexpr int N = MT::N;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
-        if (i < N - 1) y0[s] = p.Y[(long long)i * p.ncells + cell];
+        const int i = lane + MT::G * s;
+        if (i < N - 1) y0[s] = p.Y[(long long)i * p.pitch + cell];
         else if (i == N - 1) y0[s] = p.T[cell];
         else y0[s] = 0.0;
     }
@@ -155,15 +164,15 @@ __device__ __forceinline__ double cell_density(double P, const double (&y)[MT::N
     double sy = 0.0, sw = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + MT::G * s;
         if (i < N - 1) {
             sy += y[s];
             sw += y[s] * __ldg(M.inv_mw + i);
         }
     }
-    sy = warp_sum(sy);
-    sw = warp_sum(sw) + (1.0 - sy) * __ldg(M.inv_mw + N - 1);
-    const double T = __shfl_sync(kFull, y[(N - 1) / 32], (N - 1) % 32);
+    sy = group_sum<MT::G>(sy);
+    sw = group_sum<MT::G>(sw) + (1.0 - sy) * __ldg(M.inv_mw + N - 1);
+    const double T = group_shfl<MT::G>(y[(N - 1) / MT::G], (N - 1) % MT::G);
     return ode_div(P, kRU * T * sw);
 }
 
@@ -183,17 +192,17 @@ __device__ __forceinline__ void store_cell(const KParams& p, long long cell, int
     double part = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + MT::G * s;
         if (i < N - 1) part += yo[s];
     }
-    const double yN = 1.0 - warp_sum(part);
+    const double yN = 1.0 - group_sum<MT::G>(part);
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
-        if (i < N - 1) p.Y[(long long)i * p.ncells + cell] = yo[s];
+        const int i = lane + MT::G * s;
+        if (i < N - 1) p.Y[(long long)i * p.pitch + cell] = yo[s];
         else if (i == N - 1) {
             p.T[cell] = yo[s];
-            p.Y[(long long)(N - 1) * p.ncells + cell] = yN;
+            p.Y[(long long)(N - 1) * p.pitch + cell] = yN;
         }
     }
 }
@@ -216,10 +225,11 @@ __device__ __noinline__ void helper_loop(int wib, int lane) {
 #pragma unroll 1
     for (;;) {
         const long long t0 = clock64();
+        const long long idle_limit = h->idle_cycles;
         unsigned cur;
         bool idle_out = false;
         while ((cur = ld_volatile(&h->seq)) == seen) {
-            if (clock64() - t0 > kHelperIdleCycles) { idle_out = true; break; }
+            if (clock64() - t0 > idle_limit) { idle_out = true; break; }
             __nanosleep(32);
         }
         __syncwarp();
@@ -244,9 +254,10 @@ __device__ __noinline__ void helper_loop(int wib, int lane) {
 template <class MT, class LinT, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KParams p) {
     using R = StepRecord<MT, LinT>;
-    const int lane = threadIdx.x & 31;
-    const int wib = threadIdx.x >> 5;
-    long long cells_per_block = blockDim.x >> 5;
+    constexpr int G = MT::G;                 // lanes per cell
+    const int lane = threadIdx.x % G;        // lane within the cell's group
+    const int wib = threadIdx.x / G;         // the cell's slot in the CTA
+    long long cells_per_block = blockDim.x / G;
     if constexpr (MT::N >= kWideN) {
         // one cell per CTA: warp 0 integrates, warps 1-3 serve it (see HelperCtl)
         HelperCtl* hc = &g_helper_ctl;
@@ -257,7 +268,12 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
             hc->posted = 0;
             hc->cmd = 0;
             hc->err = 0;
+            hc->poisoned = 0;
+            hc->exit_posted = serve ? 0 : 1;
             hc->nhelpers = serve ? kHelperWarps : 0;
+            hc->join_cycles = p.helper_join_cycles > 0 ? p.helper_join_cycles : kJoinCycles;
+            hc->drain_cycles = p.helper_drain_cycles > 0 ? p.helper_drain_cycles : kDrainCycles;
+            hc->idle_cycles = p.helper_idle_cycles > 0 ? p.helper_idle_cycles : kHelperIdleCycles;
         }
         __syncthreads();
         if (serve) {
@@ -276,7 +292,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
     auto* wglob = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal);
     const int profiling = (p.prof != nullptr && !step_form) ? 1 : 0;
     if (lane < 8) S.prof[lane] = 0;
-    __syncwarp();
+    __syncwarp(gmask<G>());
     const long long t_start = profiling ? clock64() : 0;
     unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     long long cell = gw;
@@ -290,7 +306,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
             if (left == 0) {
                 unsigned long long c = 0;
                 if (lane == 0) c = atomicAdd(p.queue, (unsigned long long)p.chunk);
-                next = __shfl_sync(kFull, c, 0);
+                next = group_shfl<G>(c, 0);
                 left = p.chunk;
             }
             if (next >= (unsigned long long)p.ncells) break;
@@ -312,10 +328,16 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         S.lu_dirty = 0;
         int status = 0;
         bool done = false;
-        bool ill = false;   // pressure not > 0 (or NaN): CVODE's CV_ILL_INPUT, cell left as given
-        int helper_err0 = 0;
-        if constexpr (MT::N >= kWideN) helper_err0 = g_helper_ctl.err;
-        if (phase == 0) {
+        bool ill = false;   // cell left as given: pressure not > 0 (or NaN, CVODE's CV_ILL_INPUT),
+                            // or claimed by a poisoned CTA (CV_ERR_FAILURE, see HelperCtl)
+        if constexpr (MT::N >= kWideN) {
+            if (g_helper_ctl.poisoned) {
+                ill = done = true;
+                status = cv::CV_ERR_FAILURE;
+                for (int i = 0; i < 7; ++i) S.cnt[i] = 0;
+            }
+        }
+        if (!done && phase == 0) {
             Vec<MT::NS> y0;
             load_cell<MT>(p, cell, lane, y0.v);
             const double P0 = p.P ? p.P[cell] : p.P_scalar;
@@ -331,8 +353,9 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         }
         if (!done) status = bdf_advance<MT, LinT>(off, wg, p.t1, p.steps, done, lane);
         if constexpr (MT::N >= kWideN) {
-            // a helper wait ran out during this cell: its factors may be incomplete
-            if (g_helper_ctl.err != helper_err0 && status == 0) {
+            // the CTA was poisoned during this cell: late helper writes may have
+            // reached its rates or factors
+            if (g_helper_ctl.poisoned && !ill) {
                 status = cv::CV_ERR_FAILURE;
                 done = true;
             }
@@ -354,7 +377,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         if (step_form) bdf_save<MT, LinT>(off, rec, done ? 2 : 1, lane);
     }
     if constexpr (MT::N >= kWideN) {
-        if (g_helper_ctl.nhelpers == kHelperWarps) helpers_post(&g_helper_ctl, kCmdExit, lane);
+        if (!g_helper_ctl.exit_posted) helpers_post(&g_helper_ctl, kCmdExit, lane);
     }
     if (lane == 0)
         for (int i = 0; i < 8; ++i)
@@ -371,12 +394,12 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
 // outputs in the reference's layout.
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParams p, double* dTdt, double* dYdt) {
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x % MT::G, wib = threadIdx.x / MT::G;
     if constexpr (MT::N >= kWideN) {   // no helper warps here
         if (threadIdx.x == 0) g_helper_ctl.nhelpers = 0;
         __syncthreads();
     }
-    const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    const long long cell = (long long)blockIdx.x * (blockDim.x / MT::G) + wib;
     if (cell >= p.ncells) return;
     auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     Vec<MT::NS> y;
@@ -385,7 +408,7 @@ __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParam
     const Vec<MT::NS> f = warp_rhs<MT>(P, y, smem_off(&sm->chem), lane);
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + MT::G * s;
         if (i < MT::N - 1) dYdt[(long long)i * p.ncells + cell] = f.v[s];
         else if (i == MT::N - 1) dTdt[cell] = f.v[s];
     }
@@ -394,12 +417,12 @@ __global__ void __launch_bounds__(128) k_eval_rhs(const __grid_constant__ KParam
 // jac: per cell N*N column-major, reference order [T, Y_0 .. Y_{N-2}].
 template <class MT, class LinT>
 __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParams p, double* jac) {
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int lane = threadIdx.x % MT::G, wib = threadIdx.x / MT::G;
     if constexpr (MT::N >= kWideN) {   // no helper warps here
         if (threadIdx.x == 0) g_helper_ctl.nhelpers = 0;
         __syncthreads();
     }
-    const long long cell = (long long)blockIdx.x * (blockDim.x >> 5) + wib;
+    const long long cell = (long long)blockIdx.x * (blockDim.x / MT::G) + wib;
     if (cell >= p.ncells) return;
     auto* sm = reinterpret_cast<WarpSmem<MT, LinT>*>(dyn_smem()) + wib;
     auto* wg = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal) + cell;
@@ -410,7 +433,7 @@ __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParam
     constexpr int N = MT::N;
     double* out = jac + cell * (long long)(N * N);
     for (int i = 0; i < N; ++i)
-        for (int j = lane; j < N; j += 32) {   // internal row i, column j
+        for (int j = lane; j < N; j += MT::G) {   // internal row i, column j
             const int ri = (i == N - 1) ? 0 : i + 1, rj = (j == N - 1) ? 0 : j + 1;
             out[ri + N * rj] = (double)sm->A[i * MT::LDA + j];
         }
@@ -454,13 +477,38 @@ __global__ void k_fp64_peak(double* out, int iters) {
     if (r == 12345.0) out[0] = r;   // keep the chains live
 }
 
+// FP32 FMA throughput probe: independent FFMA chains per thread (the Newton
+// matrix, its LU and the triangular solves run on this pipe in mixed precision).
+__global__ void k_fp32_peak(float* out, int iters) {
+    float a0 = threadIdx.x * 1e-9f, a1 = a0 + 1e-9f, a2 = a0 + 2e-9f, a3 = a0 + 3e-9f, a4 = a0 + 4e-9f,
+          a5 = a0 + 5e-9f, a6 = a0 + 6e-9f, a7 = a0 + 7e-9f;
+    const float m = 0.999999f, c = 1e-9f;
+#pragma unroll 1
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.0f) out[0] = r;   // keep the chains live
+}
+
 // ------------------------------------------------------------------ handle
 // struct b200ode_handle: b200ode_internal.h
 
 namespace {
 
+// Shared memory of one warp: the per-cell WarpSmem of each of its 32 / G cells.
 template <class MT, class LinT>
-size_t warp_smem_bytes() { return sizeof(WarpSmem<MT, LinT>); }
+size_t warp_smem_bytes() { return sizeof(WarpSmem<MT, LinT>) * (32 / MT::G); }
+
+// Cells a CTA of wpb warps integrates at once (one per warp, or 32 / G per warp
+// for the mechanisms that put several cells in a warp; with helper warps the
+// CTA is launched as wpb = 1 and holds one cell).
+template <class MT>
+long long cells_per_block(int wpb) { return (long long)wpb * (32 / MT::G); }
 
 b200ode_status ensure_wg(b200ode_handle* h, size_t bytes) {
     if (bytes <= h->wg_bytes) return B200ODE_OK;
@@ -526,9 +574,10 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
         if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
         if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
         h->last_blocks_per_sm = bps;
+        const long long cpb = cells_per_block<MT>(wpb);
         long long blocks = (long long)bps * h->num_sms;
-        blocks = std::max(1LL, std::min(blocks, (long long)((n + wpb - 1) / wpb)));
-        b200ode_status rc = ensure_wg(h, (size_t)blocks * wpb * sizeof(WarpGlobal<MT, LinT>));
+        blocks = std::max(1LL, std::min(blocks, ((long long)n + cpb - 1) / cpb));
+        b200ode_status rc = ensure_wg(h, (size_t)(blocks * cpb) * sizeof(WarpGlobal<MT, LinT>));
         if (rc != B200ODE_OK) return rc;
         p.wglobal = h->d_wg;
         p.records = nullptr;
@@ -554,7 +603,8 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     p.wglobal = h->d_wg;
     p.records = h->d_rec;
     p.steps = 1;
-    const unsigned blocks = (unsigned)((n + wpb - 1) / wpb);
+    const long long cpb = cells_per_block<MT>(wpb);
+    const unsigned blocks = (unsigned)(((long long)n + cpb - 1) / cpb);
     const int per_check = h->opt.use_graph ? 16 : 1;
     cudaGraphExec_t gexec = nullptr;
     if (h->opt.use_graph) {
@@ -592,8 +642,15 @@ b200ode_status dispatch_form(const b200ode_handle* h, F&& f) {
     const bool fp64 = h->opt.precision == B200ODE_FP64;
     if (h->mech == MECH_GRI30) return fp64 ? f(GriF<CV>{}, double{}) : f(GriF<CV>{}, float{});
     if (h->mech == MECH_NDODECANE) return fp64 ? f(NdF<CV>{}, double{}) : f(NdF<CV>{}, float{});
-    if (h->mech == MECH_H2LI) return fp64 ? f(H2LiF<CV>{}, double{}) : f(H2LiF<CV>{}, float{});
     if (h->mech == MECH_ESTIMATE) return f(EstF<CV>{}, float{});   // FP64 refused at creation
+    const int g = h->opt.lanes_per_cell;   // resolved at creation: 32, 16 or 8 for the H2 mechanisms
+    if (h->mech == MECH_H2LI) {
+        if (g == 8) return fp64 ? f(H2LiF<CV, 8>{}, double{}) : f(H2LiF<CV, 8>{}, float{});
+        if (g == 16) return fp64 ? f(H2LiF<CV, 16>{}, double{}) : f(H2LiF<CV, 16>{}, float{});
+        return fp64 ? f(H2LiF<CV>{}, double{}) : f(H2LiF<CV>{}, float{});
+    }
+    if (g == 8) return fp64 ? f(H2F<CV, 8>{}, double{}) : f(H2F<CV, 8>{}, float{});
+    if (g == 16) return fp64 ? f(H2F<CV, 16>{}, double{}) : f(H2F<CV, 16>{}, float{});
     return fp64 ? f(H2F<CV>{}, double{}) : f(H2F<CV>{}, float{});
 }
 
@@ -624,8 +681,9 @@ b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KP
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, bdf_threads<MT>(h, wpb), smem));
     if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
     if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
+    const long long cpb = cells_per_block<MT>(wpb);
     long long b = (long long)bps * h->num_sms;
-    b = std::max(1LL, std::min(b, (n + wpb - 1) / wpb));
+    b = std::max(1LL, std::min(b, (n + cpb - 1) / cpb));
     *kern = k;
     *blocks = b;
     *wpb_out = wpb;
@@ -638,7 +696,8 @@ b200ode_status launch_eval(b200ode_handle* h, KParams& p, double* d_dT, double* 
                            cudaStream_t st) {
     const int wpb = pick_wpb<MT, LinT>(h);   // shared memory per warp decides (4 for GRI, 1-2 for larger)
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
-    const unsigned blocks = (unsigned)((p.ncells + wpb - 1) / wpb);
+    const long long cpb = cells_per_block<MT>(wpb);
+    const unsigned blocks = (unsigned)((p.ncells + cpb - 1) / cpb);
     if (d_jac) {
         b200ode_status rc = ensure_wg(h, (size_t)p.ncells * sizeof(WarpGlobal<MT, LinT>));
         if (rc != B200ODE_OK) return rc;
@@ -680,6 +739,7 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
                  double* dY, int32_t* dstat, int32_t* const* dcnt, double t0, double t1) {
     std::memset(&p, 0, sizeof(p));
     p.ncells = n;
+    p.pitch = n;
     p.P = dP;
     p.P_scalar = Ps;
     p.T = dT;
@@ -699,17 +759,71 @@ void fill_params(b200ode_handle* h, KParams& p, int64_t n, const double* dP, dou
     p.refine = h->opt.refine;
     p.chunk = std::max(1, std::min(h->opt.queue_chunk, 64));
     p.helpers = h->opt.cta_helpers != 0;
+    p.helper_join_cycles = h->opt.helper_join_cycles;
+    p.helper_drain_cycles = h->opt.helper_drain_cycles;
+    p.helper_idle_cycles = h->opt.helper_idle_cycles;
 }
 
-b200ode_status read_totals(b200ode_handle* h, b200ode_stats* s, cudaStream_t st) {
+// Device bytes per cell a launch of this handle needs beyond the caller's
+// buffers: the one-launch-per-step form keeps a state record and a
+// WarpGlobal per cell; the persistent form only per resident warp.
+size_t step_form_bytes_per_cell(const b200ode_handle* h) {
+    if (h->opt.persistent) return 0;
+    size_t b = 0;
+    dispatch_mech(h, [&](auto mt, auto lt) {
+        using MT = decltype(mt);
+        using LinT = decltype(lt);
+        b = StepRecord<MT, LinT>::kBytes + sizeof(WarpGlobal<MT, LinT>);
+        return B200ODE_OK;
+    });
+    return b;
+}
+
+// Cells per launch: the whole batch when it fits, else memory-sized chunks
+// (the reference's calc_gpu_points, src/Integrators/Drivers/CVodeGPUDriver.cu:108-130,
+// takes 80 % of the free memory over its per-cell footprint the same way).
+// io_bytes_per_cell: the handle's own I/O buffers (host-buffer entry point) or
+// 0 (caller's device buffers).  `held` = bytes the handle already holds for
+// these buffers (freed and re-allocated when they grow).
+int64_t cells_per_launch(const b200ode_handle* h, int64_t n, size_t io_bytes_per_cell) {
+    if (n <= 0) return 1;
+    int64_t limit = n;
+    if (h->opt.max_cells_per_launch > 0) limit = std::min<int64_t>(limit, h->opt.max_cells_per_launch);
+    const size_t per_cell = step_form_bytes_per_cell(h) + io_bytes_per_cell;
+    if (per_cell > 0) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+            const size_t held = h->rec_bytes + (h->opt.persistent ? 0 : h->wg_bytes) +
+                                h->cap * io_bytes_per_cell;
+            const double avail = 0.8 * (double)(free_b + held);
+            int64_t fit = (int64_t)(avail / (double)per_cell);
+            if (fit >= 64) fit -= fit % 32;
+            limit = std::min<int64_t>(limit, std::max<int64_t>(fit, 1));
+        } else {
+            cudaGetLastError();
+        }
+    }
+    return std::max<int64_t>(limit, 1);
+}
+
+// Adds one launch's call totals (read from the control block) into *s.
+b200ode_status add_totals(b200ode_handle* h, const unsigned long long* ctl, b200ode_stats* s, cudaStream_t st) {
     unsigned long long t[15];
-    CUDA_TRY(cudaMemcpyAsync(t, h->d_ctl + 1, sizeof(t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(t, ctl + 1, sizeof(t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    for (int i = 0; i < 5; ++i) s->phase_cycles[i] = h->opt.profile_phases ? (int64_t)t[9 + i] : 0;
-    s->total_nst = (int64_t)t[0]; s->total_nfe = (int64_t)t[1]; s->total_nje = (int64_t)t[2];
-    s->total_nsetups = (int64_t)t[3]; s->total_nni = (int64_t)t[4]; s->total_ncfn = (int64_t)t[5];
-    s->total_netf = (int64_t)t[6]; s->n_failed = (int64_t)t[7];
+    for (int i = 0; i < 5; ++i) s->phase_cycles[i] += h->opt.profile_phases ? (int64_t)t[9 + i] : 0;
+    s->total_nst += (int64_t)t[0]; s->total_nfe += (int64_t)t[1]; s->total_nje += (int64_t)t[2];
+    s->total_nsetups += (int64_t)t[3]; s->total_nni += (int64_t)t[4]; s->total_ncfn += (int64_t)t[5];
+    s->total_netf += (int64_t)t[6]; s->n_failed += (int64_t)t[7];
     return B200ODE_OK;
+}
+
+// Zeroes the totals and timings of *s, keeping its per-cell counter pointers.
+void clear_totals(b200ode_stats* s) {
+    int32_t* keep[7] = {s->nst, s->nfe, s->nje, s->nsetups, s->nni, s->ncfn, s->netf};
+    std::memset(s, 0, sizeof(*s));
+    s->nst = keep[0]; s->nfe = keep[1]; s->nje = keep[2]; s->nsetups = keep[3];
+    s->nni = keep[4]; s->ncfn = keep[5]; s->netf = keep[6];
 }
 
 }  // namespace
@@ -729,7 +843,7 @@ size_t persistent_scratch_bytes(b200ode_handle* h, int64_t n) {
         int wpb = 0;
         size_t smem = 0;
         b200ode_status rc = persistent_shape<MT, LinT>(h, std::max<long long>(n, 1), &k, &blocks, &wpb, &smem);
-        if (rc == B200ODE_OK) bytes = (size_t)blocks * wpb * sizeof(WarpGlobal<MT, LinT>);
+        if (rc == B200ODE_OK) bytes = (size_t)(blocks * cells_per_block<MT>(wpb)) * sizeof(WarpGlobal<MT, LinT>);
         return rc;
     });
     return bytes;
@@ -786,6 +900,11 @@ void b200ode_default_options(b200ode_options* o) {
     o->profile_phases = 0;
     o->formulation = B200ODE_CONP;
     o->cta_helpers = 1;
+    o->helper_join_cycles = 0;
+    o->helper_drain_cycles = 0;
+    o->helper_idle_cycles = 0;
+    o->max_cells_per_launch = 0;
+    o->lanes_per_cell = 0;
 }
 
 const char* b200ode_last_error(void) { return g_last_error.c_str(); }
@@ -825,6 +944,12 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
         return fail(B200ODE_ERR_INVALID, "precision must be B200ODE_FP64 or B200ODE_MIXED");
     if (o.formulation != B200ODE_CONP && o.formulation != B200ODE_CONV)
         return fail(B200ODE_ERR_INVALID, "formulation must be B200ODE_CONP or B200ODE_CONV");
+    // lanes per cell: 32 (a warp per cell) for every mechanism; the two H2
+    // mechanisms (9-10 unknowns) also run 2 or 4 cells per warp
+    const bool small_mech = (mech == MECH_H2O2 || mech == MECH_H2LI);
+    if (o.lanes_per_cell == 0) o.lanes_per_cell = small_mech ? kSmallMechLanes : 32;
+    if (o.lanes_per_cell != 32 && !(small_mech && (o.lanes_per_cell == 16 || o.lanes_per_cell == 8)))
+        return fail(B200ODE_ERR_INVALID, "lanes_per_cell must be 0 or 32 (or 16 / 8 for h2o2 and h2_li_2004)");
     if (mech == MECH_ESTIMATE && o.precision == B200ODE_FP64)
         return fail(B200ODE_ERR_INVALID,
                     "ESTiMatE-Mech_04042022 (214 unknowns) runs in B200ODE_MIXED only: its FP64 Newton "
@@ -915,30 +1040,41 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n, const doub
     NvtxRange range("b200ode_integrate_device");
     b200ode_status rc = check_args(h, n, t0, t1);
     if (rc != B200ODE_OK) return rc;
-    if (n == 0) {
-        if (stats) { std::memset(stats, 0, sizeof(*stats)); }
-        return B200ODE_OK;
-    }
+    if (stats) clear_totals(stats);
+    if (n == 0) return B200ODE_OK;
     if (!dT || !dY) return fail(B200ODE_ERR_INVALID, "null T or Y");
     cudaStream_t st = (cudaStream_t)stream;
-    int32_t* dcnt[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    int32_t* cnt[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (stats) {
         int32_t* src[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
-        for (int i = 0; i < 7; ++i) dcnt[i] = src[i];
+        for (int i = 0; i < 7; ++i) cnt[i] = src[i];
     }
-    KParams p;
-    fill_params(h, p, n, dP, Ps, dT, dY, dstat, dcnt, t0, t1);
+    // memory-sized chunks (one launch sequence each; the step form's per-cell
+    // records would otherwise outgrow the device for very large batches)
+    const int64_t chunk = cells_per_launch(h, n, 0);
     int launches = 0;
-    CUDA_TRY(cudaEventRecord(h->ev[1], st));
-    rc = run(h, p, st, &launches);
-    if (rc != B200ODE_OK) return rc;
-    CUDA_TRY(cudaEventRecord(h->ev[2], st));
-    if (stats) {
-        rc = read_totals(h, stats, st);
+    float kernel_ms = 0.f;
+    for (int64_t a = 0; a < n; a += chunk) {
+        const int64_t m = std::min(chunk, n - a);
+        int32_t* dcnt[7];
+        for (int i = 0; i < 7; ++i) dcnt[i] = cnt[i] ? cnt[i] + a : nullptr;
+        KParams p;
+        fill_params(h, p, m, dP ? dP + a : nullptr, Ps, dT + a, dY + a, dstat ? dstat + a : nullptr, dcnt, t0, t1);
+        p.pitch = n;
+        CUDA_TRY(cudaEventRecord(h->ev[1], st));
+        rc = run(h, p, st, &launches);
         if (rc != B200ODE_OK) return rc;
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
-        stats->kernel_ms = ms;
+        CUDA_TRY(cudaEventRecord(h->ev[2], st));
+        if (stats) {
+            rc = add_totals(h, h->d_ctl, stats, st);
+            if (rc != B200ODE_OK) return rc;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
+            kernel_ms += ms;
+        }
+    }
+    if (stats) {
+        stats->kernel_ms = kernel_ms;
         stats->h2d_ms = stats->d2h_ms = 0.0;
         stats->gpu_launches = launches;
     }
@@ -951,65 +1087,75 @@ b200ode_status b200ode_integrate(b200ode_handle* h, int64_t n, const double* P, 
     NvtxRange range("b200ode_integrate");
     b200ode_status rc = check_args(h, n, t0, t1);
     if (rc != B200ODE_OK) return rc;
-    if (n == 0) {
-        if (stats) {
-            int32_t* keep[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
-            std::memset(stats, 0, sizeof(*stats));
-            stats->nst = keep[0]; stats->nfe = keep[1]; stats->nje = keep[2]; stats->nsetups = keep[3];
-            stats->nni = keep[4]; stats->ncfn = keep[5]; stats->netf = keep[6];
-        }
-        return B200ODE_OK;
-    }
+    if (stats) clear_totals(stats);
+    if (n == 0) return B200ODE_OK;
     if (!T || !Y) return fail(B200ODE_ERR_INVALID, "null T or Y");
     if (!P && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
-    rc = ensure_cap(h, (size_t)n);
+    const size_t nsp = h->hm.nsp;
+    // the handle's device buffers hold one chunk: the whole batch when it fits
+    // in device memory, else memory-sized chunks copied in and out in turn
+    const size_t io_per_cell = (nsp + 2) * sizeof(double) + 8 * sizeof(int32_t);
+    const int64_t chunk = cells_per_launch(h, n, io_per_cell);
+    rc = ensure_cap(h, (size_t)chunk);
     if (rc != B200ODE_OK) return rc;
     cudaStream_t st = h->stream;
-    const size_t nsp = h->hm.nsp;
     const bool want_cnt = stats && (stats->nst || stats->nfe || stats->nje || stats->nsetups ||
                                     stats->nni || stats->ncfn || stats->netf);
-    {
-    NvtxRange h2d_range("h2d");
-    CUDA_TRY(cudaEventRecord(h->ev[0], st));
-    CUDA_TRY(cudaMemcpyAsync(h->d_T, T, n * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(h->d_Y, Y, n * nsp * sizeof(double), cudaMemcpyHostToDevice, st));
-    if (P) CUDA_TRY(cudaMemcpyAsync(h->d_P, P, n * sizeof(double), cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaEventRecord(h->ev[1], st));
-    }
-    int32_t* dcnt[7];
-    for (int i = 0; i < 7; ++i) dcnt[i] = want_cnt ? h->d_cnt + (size_t)i * n : nullptr;
-    KParams p;
-    fill_params(h, p, n, P ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, h->d_status, dcnt, t0, t1);
-    int launches = 0;
-    rc = run(h, p, st, &launches);
-    if (rc != B200ODE_OK) return rc;
-    CUDA_TRY(cudaEventRecord(h->ev[2], st));
-    CUDA_TRY(cudaMemcpyAsync(T, h->d_T, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(Y, h->d_Y, n * nsp * sizeof(double), cudaMemcpyDeviceToHost, st));
-    if (cell_status)
-        CUDA_TRY(cudaMemcpyAsync(cell_status, h->d_status, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    int32_t* dst[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (want_cnt) {
-        int32_t* dst[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+        int32_t* d[7] = {stats->nst, stats->nfe, stats->nje, stats->nsetups, stats->nni, stats->ncfn, stats->netf};
+        for (int i = 0; i < 7; ++i) dst[i] = d[i];
+    }
+    int launches = 0;
+    float t_h2d = 0.f, t_kernel = 0.f, t_d2h = 0.f;
+    for (int64_t a = 0; a < n; a += chunk) {
+        const int64_t m = std::min(chunk, n - a);
+        {
+            NvtxRange h2d_range("h2d");
+            CUDA_TRY(cudaEventRecord(h->ev[0], st));
+            CUDA_TRY(cudaMemcpyAsync(h->d_T, T + a, m * sizeof(double), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpy2DAsync(h->d_Y, m * sizeof(double), Y + a, n * sizeof(double), m * sizeof(double),
+                                       nsp, cudaMemcpyHostToDevice, st));
+            if (P) CUDA_TRY(cudaMemcpyAsync(h->d_P, P + a, m * sizeof(double), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaEventRecord(h->ev[1], st));
+        }
+        int32_t* dcnt[7];
+        for (int i = 0; i < 7; ++i) dcnt[i] = want_cnt ? h->d_cnt + (size_t)i * m : nullptr;
+        KParams p;
+        fill_params(h, p, m, P ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, h->d_status, dcnt, t0, t1);
+        rc = run(h, p, st, &launches);
+        if (rc != B200ODE_OK) return rc;
+        CUDA_TRY(cudaEventRecord(h->ev[2], st));
+        CUDA_TRY(cudaMemcpyAsync(T + a, h->d_T, m * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpy2DAsync(Y + a, n * sizeof(double), h->d_Y, m * sizeof(double), m * sizeof(double), nsp,
+                                   cudaMemcpyDeviceToHost, st));
+        if (cell_status)
+            CUDA_TRY(cudaMemcpyAsync(cell_status + a, h->d_status, m * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         for (int i = 0; i < 7; ++i)
             if (dst[i])
-                CUDA_TRY(cudaMemcpyAsync(dst[i], h->d_cnt + (size_t)i * n, n * sizeof(int32_t),
+                CUDA_TRY(cudaMemcpyAsync(dst[i] + a, h->d_cnt + (size_t)i * m, m * sizeof(int32_t),
                                          cudaMemcpyDeviceToHost, st));
-    }
-    CUDA_TRY(cudaEventRecord(h->ev[3], st));
-    {
-        NvtxRange wait("device (copies + BDF kernel)");
-        CUDA_TRY(cudaStreamSynchronize(st));
+        CUDA_TRY(cudaEventRecord(h->ev[3], st));
+        {
+            NvtxRange wait("device (copies + BDF kernel)");
+            CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        if (stats) {
+            rc = add_totals(h, h->d_ctl, stats, st);
+            if (rc != B200ODE_OK) return rc;
+            float x = 0.f, y = 0.f, z = 0.f;
+            cudaEventElapsedTime(&x, h->ev[0], h->ev[1]);
+            cudaEventElapsedTime(&y, h->ev[1], h->ev[2]);
+            cudaEventElapsedTime(&z, h->ev[2], h->ev[3]);
+            t_h2d += x;
+            t_kernel += y;
+            t_d2h += z;
+        }
     }
     if (stats) {
-        rc = read_totals(h, stats, st);
-        if (rc != B200ODE_OK) return rc;
-        float a = 0.f, b = 0.f, c = 0.f;
-        cudaEventElapsedTime(&a, h->ev[0], h->ev[1]);
-        cudaEventElapsedTime(&b, h->ev[1], h->ev[2]);
-        cudaEventElapsedTime(&c, h->ev[2], h->ev[3]);
-        stats->h2d_ms = a;
-        stats->kernel_ms = b;
-        stats->d2h_ms = c;
+        stats->h2d_ms = t_h2d;
+        stats->kernel_ms = t_kernel;
+        stats->d2h_ms = t_d2h;
         stats->gpu_launches = launches;
     }
     return B200ODE_OK;
@@ -1105,20 +1251,17 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     if (rc != B200ODE_OK) return rc;
     if (n <= 0 || !dT || !dY) return fail(B200ODE_ERR_INVALID, "autotune needs cells (device T and Y)");
     if (!dP && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
-    const int64_t m = std::min<int64_t>(n, 8192);
+    const bool small_mech = (h->mech == MECH_H2O2 || h->mech == MECH_H2LI);
+    const bool wide_mech = (h->mech == MECH_ESTIMATE);   // one cell per SM: helper warps on or off
+    // the sample: the first m cells (a few per SM for the widest mechanism, whose
+    // cells take seconds), copied so the caller's buffers stay untouched
+    const int64_t m = std::min<int64_t>(n, wide_mech ? 2 * (int64_t)h->num_sms : 8192);
     const size_t nsp = h->hm.nsp;
     rc = ensure_cap(h, (size_t)m);
     if (rc != B200ODE_OK) return rc;
     cudaStream_t st = h->stream;
-    // shared memory per warp, against a CTA's limit (shapes that exceed it are skipped)
-    size_t warp_smem = 0;
-    dispatch_mech(h, [&](auto mt, auto lt) {
-        warp_smem = warp_smem_bytes<decltype(mt), decltype(lt)>();
-        return B200ODE_OK;
-    });
     int smem_optin = 0;
     CUDA_TRY(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-    // the sample: the first m cells, copied so the caller's buffers stay untouched
     double *sT = nullptr, *sY = nullptr;
     CUDA_TRY(cudaMallocAsync(&sT, m * sizeof(double), st));
     CUDA_TRY(cudaMallocAsync(&sY, m * nsp * sizeof(double), st));
@@ -1127,40 +1270,85 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
                                cudaMemcpyDeviceToDevice, st));
     if (dP) CUDA_TRY(cudaMemcpyAsync(h->d_P, dP, m * sizeof(double), cudaMemcpyDeviceToDevice, st));
     const b200ode_options saved = h->opt;
-    // warps per CTA x register variant (blocks_per_sm >= 3 * 4 / wpb selects the
-    // 168-register variant, which trades spills for resident warps); shapes
-    // whose shared memory exceeds a CTA's (e.g. 4 or 2 warps of the 214-species
-    // mechanism) are skipped
-    const int cand[6][2] = {{4, 0}, {2, 0}, {1, 0}, {4, 3}, {2, 6}, {1, 12}};
-    float best_ms = 0.f;
-    int best = -1;
     h->opt.persistent = 1;
-    for (int c = 0; c < 6 && rc == B200ODE_OK; ++c) {
-        if ((size_t)cand[c][0] * warp_smem > (size_t)smem_optin) continue;
-        h->opt.warps_per_block = cand[c][0];
-        h->opt.blocks_per_sm = cand[c][1];
+    // best of two timed persistent runs of the sample under the handle's current options
+    auto time_opts = [&](float* out_ms) -> b200ode_status {
         float ms_c = 1e30f;
-        for (int rep = 0; rep < 2 && rc == B200ODE_OK; ++rep) {
+        for (int rep = 0; rep < 2; ++rep) {
             if (cudaMemcpyAsync(h->d_T, sT, m * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-                cudaMemcpyAsync(h->d_Y, sY, m * nsp * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess) {
-                rc = fail(B200ODE_ERR_CUDA, "autotune: sample copy");
-                break;
-            }
+                cudaMemcpyAsync(h->d_Y, sY, m * nsp * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+                return fail(B200ODE_ERR_CUDA, "autotune: sample copy");
             KParams p;
             fill_params(h, p, m, dP ? h->d_P : nullptr, Ps, h->d_T, h->d_Y, h->d_status, nullptr, t0, t1);
             int launches = 0;
-            if (cudaEventRecord(h->ev[1], st) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "event"); break; }
-            rc = run(h, p, st, &launches);
-            if (rc != B200ODE_OK) break;
+            if (cudaEventRecord(h->ev[1], st) != cudaSuccess) return fail(B200ODE_ERR_CUDA, "event");
+            b200ode_status r = run(h, p, st, &launches);
+            if (r != B200ODE_OK) return r;
             cudaEventRecord(h->ev[2], st);
-            if (cudaEventSynchronize(h->ev[2]) != cudaSuccess) { rc = fail(B200ODE_ERR_CUDA, "autotune run"); break; }
+            if (cudaEventSynchronize(h->ev[2]) != cudaSuccess) return fail(B200ODE_ERR_CUDA, "autotune run");
             float ms = 0.f;
             cudaEventElapsedTime(&ms, h->ev[1], h->ev[2]);
             ms_c = std::min(ms_c, ms);
         }
-        if (rc == B200ODE_OK && (best < 0 || ms_c < best_ms)) {
-            best_ms = ms_c;
+        *out_ms = ms_c;
+        return B200ODE_OK;
+    };
+    // stage 1, the launch shape: lanes per cell (32, or 16 / 8 for the H2
+    // mechanisms) x warps per CTA (4, 2, 1) x register variant (blocks_per_sm >=
+    // 3 * 4 / wpb selects the 168-register variant, which trades spills for
+    // resident warps) x helper warps (widest mechanism); shapes whose shared
+    // memory exceeds a CTA's are skipped
+    struct Cand { int lanes, wpb, bps, helpers, chunk; };
+    std::vector<Cand> shapes;
+    for (int lanes : {32, 16, 8}) {
+        if (lanes != 32 && !small_mech) continue;
+        for (int wpb : {4, 2, 1})
+            for (int v = 0; v < 2; ++v)
+                for (int helpers : {1, 0}) {
+                    if (helpers == 0 && !(wide_mech && wpb == 1)) continue;
+                    shapes.push_back({lanes, wpb, v ? 3 * (4 / wpb) : 0, helpers, 1});
+                }
+    }
+    float best_ms = 0.f;
+    Cand best{0, 0, 0, 0, 0};
+    bool have = false;
+    for (const Cand& c : shapes) {
+        if (rc != B200ODE_OK) break;
+        h->opt.lanes_per_cell = c.lanes;
+        h->opt.warps_per_block = c.wpb;
+        h->opt.blocks_per_sm = c.bps;
+        h->opt.cta_helpers = c.helpers;
+        h->opt.queue_chunk = 1;
+        size_t warp_smem = 0;
+        dispatch_mech(h, [&](auto mt, auto lt) {
+            warp_smem = warp_smem_bytes<decltype(mt), decltype(lt)>();
+            return B200ODE_OK;
+        });
+        if ((size_t)c.wpb * warp_smem > (size_t)smem_optin) continue;
+        float ms = 0.f;
+        rc = time_opts(&ms);
+        if (rc == B200ODE_OK && (!have || ms < best_ms)) {
+            best_ms = ms;
             best = c;
+            have = true;
+        }
+    }
+    // stage 2, the work-queue chunk (cells a warp claims per queue access) on
+    // the chosen shape
+    if (rc == B200ODE_OK && have) {
+        h->opt.lanes_per_cell = best.lanes;
+        h->opt.warps_per_block = best.wpb;
+        h->opt.blocks_per_sm = best.bps;
+        h->opt.cta_helpers = best.helpers;
+        for (int chunk : {2, 8}) {
+            h->opt.queue_chunk = chunk;
+            float ms = 0.f;
+            rc = time_opts(&ms);
+            if (rc != B200ODE_OK) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.chunk = chunk;
+            }
         }
     }
     cudaFreeAsync(sT, st);
@@ -1168,11 +1356,48 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     cudaStreamSynchronize(st);
     h->opt = saved;
     if (rc != B200ODE_OK) return rc;
-    if (best < 0) return fail(B200ODE_ERR_CUDA, "autotune: no launch shape fits this device");
-    h->opt.warps_per_block = cand[best][0];
-    h->opt.blocks_per_sm = cand[best][1];
-    if (wpb_out) *wpb_out = cand[best][0];
-    if (bps_out) *bps_out = cand[best][1];
+    if (!have) return fail(B200ODE_ERR_CUDA, "autotune: no launch shape fits this device");
+    h->opt.lanes_per_cell = best.lanes;
+    h->opt.warps_per_block = best.wpb;
+    h->opt.blocks_per_sm = best.bps;
+    h->opt.cta_helpers = best.helpers;
+    h->opt.queue_chunk = best.chunk;
+    if (wpb_out) *wpb_out = best.wpb;
+    if (bps_out) *bps_out = best.bps;
+    return B200ODE_OK;
+}
+
+b200ode_status b200ode_get_options(const b200ode_handle* h, b200ode_options* out) {
+    if (!h || !out) return fail(B200ODE_ERR_INVALID, "null handle or output");
+    *out = h->opt;
+    return B200ODE_OK;
+}
+
+b200ode_status b200ode_fp32_peak(int32_t device, double* gflops) {
+    if (!gflops) return fail(B200ODE_ERR_INVALID, "null output");
+    if (device >= 0) CUDA_TRY(cudaSetDevice(device));
+    int dev = 0, sms = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    float* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(float)));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 4096, threads = 256, blocks = sms * 8;
+    k_fp32_peak<<<blocks, threads>>>(d, 16);
+    cudaEventRecord(a);
+    k_fp32_peak<<<blocks, threads>>>(d, iters);
+    cudaEventRecord(b);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(B200ODE_ERR_CUDA, cudaGetErrorString(e));
+    const double flops = 2.0 * 8.0 * 16.0 * iters * (double)threads * blocks;
+    *gflops = flops / (ms * 1e-3) / 1e9;
     return B200ODE_OK;
 }
 
@@ -1265,8 +1490,12 @@ struct NoAllocDeviceGuard {
     ~NoAllocDeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
 };
 
-// Same launch shape as the persistent branch of launch_bdf (so both entry points
-// run identical grids), with queue, totals and per-warp scratch in the array.
+// Same launch shape as the persistent branch of launch_bdf -- CTA size from
+// bdf_threads (one 128-thread CTA per cell when the widest mechanisms' helper
+// warps serve), blocks from occupancy -- so both entry points run identical
+// grids, with queue, totals and per-warp scratch in the array.  With helper
+// warps the per-cell scratch index is the CTA index (one cell per CTA), so the
+// scratch stays blocks x wpb WarpGlobals.
 template <class MT, class LinT>
 b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* scratch, cudaStream_t st,
                                   int* launches) {
@@ -1276,19 +1505,21 @@ b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* 
     auto kern = k_bdf<MT, LinT, 1>;
     if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int threads = bdf_threads<MT>(h, wpb);
     int bps = 0;
-    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, wpb * 32, smem));
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, threads, smem));
     if (bps < 1) return fail(B200ODE_ERR_CUDA, "kernel does not fit on an SM");
     if (h->opt.blocks_per_sm > 0) bps = std::min(bps, h->opt.blocks_per_sm);
     const size_t n = (size_t)p.ncells;
+    const long long cpb = cells_per_block<MT>(wpb);
     long long blocks = (long long)bps * h->num_sms;
-    blocks = std::max(1LL, std::min(blocks, (long long)((n + wpb - 1) / wpb)));
-    const size_t need = kNoAllocCtlBytes + (size_t)blocks * wpb * sizeof(WG);
+    blocks = std::max(1LL, std::min(blocks, ((long long)n + cpb - 1) / cpb));
+    const size_t need = kNoAllocCtlBytes + (size_t)(blocks * cpb) * sizeof(WG);
     if (need > (size_t)B200ODE_NOALLOC_SCRATCH_BYTES)
         return fail(B200ODE_ERR_INVALID,
                     "b200ode_integrate_device_noalloc: this launch needs " + std::to_string(need) +
-                        " bytes of scratch (" + std::to_string(blocks) + " blocks x " + std::to_string(wpb) +
-                        " warps x " + std::to_string(sizeof(WG)) + " bytes + 256) but the static scratch holds " +
+                        " bytes of scratch (" + std::to_string(blocks) + " blocks x " + std::to_string(cpb) +
+                        " cells x " + std::to_string(sizeof(WG)) + " bytes + 256) but the static scratch holds " +
                         std::to_string((size_t)B200ODE_NOALLOC_SCRATCH_BYTES) +
                         " bytes; lower options.blocks_per_sm or options.warps_per_block");
     h->last_blocks_per_sm = bps;
@@ -1301,7 +1532,7 @@ b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* 
     p.wglobal = scratch + kNoAllocCtlBytes;
     p.records = nullptr;
     p.steps = 0x7fffffff;
-    kern<<<(unsigned)blocks, wpb * 32, smem, st>>>(p);
+    kern<<<(unsigned)blocks, threads, smem, st>>>(p);
     CUDA_TRY(cudaGetLastError());
     *launches += 1;
     return B200ODE_OK;

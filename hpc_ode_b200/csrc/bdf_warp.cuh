@@ -23,7 +23,7 @@
 // tau, counters) and the Nordsieck history live in the warp's shared memory;
 // every lane computes the same scalar values and writes them (identical
 // values, so the shared words are consistent).  Work vectors (ewt, acor, y,
-// ftemp, delta) are lane registers (element i = lane + 32 s; internal order
+// ftemp, delta) are lane registers (element i = lane + G s; internal order
 // Y_0..Y_{N-2}, T).  Only the Newton loop is inlined; step-size/order
 // selection, coefficient updates, the linear-solver setup, the initial step and
 // the HBM record I/O are single out-of-line copies addressed by a shared-memory
@@ -73,7 +73,7 @@ struct BdfState {
 template <class MT, class LinT>
 struct WarpSmem {
     ChemSmem<MT> chem;
-    double zn[cv::QMAX + 1][32 * MT::NS];   // Nordsieck history zn[j][i]
+    double zn[cv::QMAX + 1][MT::G * MT::NS];   // Nordsieck history zn[j][i]
     BdfState st;
     LinT A[MT::N * MT::LDA];                // Jacobian, then the LU factors of M = I - gamma J
     LinT dinv[MT::N];
@@ -93,26 +93,27 @@ __device__ __forceinline__ WarpSmem<MT, LinT>* wsm(unsigned off) {
     return smem_at<WarpSmem<MT, LinT>>(off);
 }
 
-template <int NS>
-__device__ __forceinline__ bool valid_el(int lane, int s, int N) { return lane + 32 * s < N; }
+template <int G>
+__device__ __forceinline__ bool valid_el(int lane, int s, int N) { return lane + G * s < N; }
 
-// sqrt(sum over the warp of acc / n): the tail of every WRMS norm, out of line.
-__device__ __noinline__ double wrms_reduce(double acc, int n) { return sqrt(warp_sum(acc) / n); }
+// sqrt(sum over the cell's lanes of acc / n): the tail of every WRMS norm, out of line.
+template <int G>
+__device__ __noinline__ double wrms_reduce(double acc, int n) { return sqrt(group_sum<G>(acc) / n); }
 
-template <int NS>
+template <int NS, int G>
 __device__ __forceinline__ double wrms_v(const double (&x)[NS], const double (&w)[NS], int N) {
     double acc = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) { const double t = x[s] * w[s]; acc += t * t; }
-    return wrms_reduce(acc, N);
+    return wrms_reduce<G>(acc, N);
 }
 
 template <class MT, class LinT>
 __device__ __forceinline__ double wrms_zn(const WarpSmem<MT, LinT>* w, int j, const double (&ewt)[MT::NS], int lane) {
     double acc = 0.0;
 #pragma unroll
-    for (int s = 0; s < MT::NS; ++s) { const double t = w->zn[j][lane + 32 * s] * ewt[s]; acc += t * t; }
-    return wrms_reduce(acc, MT::N);
+    for (int s = 0; s < MT::NS; ++s) { const double t = w->zn[j][lane + MT::G * s] * ewt[s]; acc += t * t; }
+    return wrms_reduce<MT::G>(acc, MT::N);
 }
 
 __device__ __forceinline__ long long ph_tick(const BdfState& S) { return S.profiling ? clock64() : 0; }
@@ -146,7 +147,7 @@ __device__ __forceinline__ void bdf_rescale(unsigned off, int lane) {
 #pragma unroll 1
     for (int j = 1; j <= q; ++j) {
 #pragma unroll
-        for (int s = 0; s < MT::NS; ++s) w->zn[j][lane + 32 * s] *= factor;
+        for (int s = 0; s < MT::NS; ++s) w->zn[j][lane + MT::G * s] *= factor;
         factor *= eta;
     }
     S.h = S.hscale * eta;
@@ -164,7 +165,7 @@ __device__ __forceinline__ void bdf_pascal(unsigned off, int lane, bool forward)
         for (int j = q; j >= k; --j)
 #pragma unroll
             for (int s = 0; s < MT::NS; ++s) {
-                const int i = lane + 32 * s;
+                const int i = lane + MT::G * s;
                 w->zn[j - 1][i] = forward ? w->zn[j - 1][i] + w->zn[j][i] : w->zn[j - 1][i] - w->zn[j][i];
             }
 }
@@ -198,7 +199,7 @@ __device__ __noinline__ void bdf_adjust_order(unsigned off, int dq, int lane) {
         const int L = S.L, ia = S.indx_acor;
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) {
-            const int i = lane + 32 * s;
+            const int i = lane + MT::G * s;
             const double col = A1 * w->zn[ia][i];
             w->zn[L][i] = col;
             #pragma unroll 1
@@ -215,7 +216,7 @@ __device__ __noinline__ void bdf_adjust_order(unsigned off, int dq, int lane) {
         }
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s) {
-            const int i = lane + 32 * s;
+            const int i = lane + MT::G * s;
             const double zq = w->zn[q][i];
             #pragma unroll 1
             for (int j = 2; j < q; ++j) w->zn[j][i] += -l[j] * zq;
@@ -303,7 +304,7 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
 #pragma unroll 1
         for (int i = 0; i < N; ++i)
             #pragma unroll 1
-            for (int j = lane; j < N; j += 32) A[i * LDA + j] = J[i * N + j];
+            for (int j = lane; j < N; j += MT::G) A[i * LDA + j] = J[i * N + j];
     } else {
         S.cnt[C_NJE]++;
         S.nstlj = S.nst;
@@ -314,19 +315,19 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
 #pragma unroll 1
         for (int i = 0; i < N; ++i)
             #pragma unroll 1
-            for (int j = lane; j < N; j += 32) J[i * N + j] = A[i * LDA + j];
+            for (int j = lane; j < N; j += MT::G) J[i * N + j] = A[i * LDA + j];
     }
-    __syncwarp();
+    __syncwarp(gmask<MT::G>());
     const LinT mg = (LinT)(-S.gamma);
 #pragma unroll 1
     for (int i = 0; i < N; ++i)
         #pragma unroll 1
-        for (int j = lane; j < N; j += 32) {
+        for (int j = lane; j < N; j += MT::G) {
             LinT v = mg * A[i * LDA + j];
             if (i == j) v += LinT(1);
             A[i * LDA + j] = v;
         }
-    __syncwarp();
+    __syncwarp(gmask<MT::G>());
     S.lu_dirty = 1;
     const long long tl = ph_tick(S);
     const int r = warp_lu<MT, LinT>(smem_off(A), smem_off(w->perm), smem_off(w->dinv), lane);
@@ -359,11 +360,11 @@ __device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], con
         for (int s = 0; s < NS; ++s) r.v[s] = a.v[s] - x.v[s];
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            const int i = lane + 32 * s;
+            const int i = lane + MT::G * s;
             double acc = 0.0;
 #pragma unroll 1
             for (int j = 0; j < N; ++j) {
-                const double xj = __shfl_sync(kFull, pick<NS>(x.v, j >> 5), j & 31);
+                const double xj = group_shfl<MT::G>(pick<NS>(x.v, j / MT::G), j % MT::G);
                 if (i < N) acc += (double)wg->savedJ[i * N + j] * xj;
             }
             if (i < N) r.v[s] += S.gammap * acc;
@@ -411,8 +412,8 @@ __device__ __noinline__ void bdf_prepare_next_step(unsigned off, double dsm, con
             const double cquot = ode_div(S.tq[5], S.saved_tq5) * ode_pow(ode_div(S.h, S.tau[2]), (double)L);
             double tmp[NS];
 #pragma unroll
-            for (int s = 0; s < NS; ++s) tmp[s] = acv.v[s] - cquot * w->zn[S.qmax][lane + 32 * s];
-            const double dup = wrms_v<NS>(tmp, ewv.v, MT::N) * S.tq[3];
+            for (int s = 0; s < NS; ++s) tmp[s] = acv.v[s] - cquot * w->zn[S.qmax][lane + MT::G * s];
+            const double dup = wrms_v<NS, MT::G>(tmp, ewv.v, MT::N) * S.tq[3];
             etaqp1 = ode_div(1.0, ode_pow(cv::BIAS3 * dup, ode_div(1.0, (double)(L + 1))) + cv::ADDON);
         }
         S.etaqm1 = etaqm1;
@@ -430,7 +431,7 @@ __device__ __noinline__ void bdf_prepare_next_step(unsigned off, double dsm, con
             eta = etaqp1;
             qprime = q + 1;
 #pragma unroll
-            for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + 32 * s] = acv.v[s];
+            for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + MT::G * s] = acv.v[s];
         }
     }
     S.qprime = qprime;
@@ -479,10 +480,10 @@ __device__ __noinline__ int bdf_error_fail(unsigned off, double dsm, double save
     S.qwait = cv::LONG_WAIT;
     double z0[MT::NS], f[MT::NS];
 #pragma unroll
-    for (int s = 0; s < MT::NS; ++s) z0[s] = w->zn[0][lane + 32 * s];
+    for (int s = 0; s < MT::NS; ++s) z0[s] = w->zn[0][lane + MT::G * s];
     bdf_rhs<MT, LinT>(off, z0, f, lane);
 #pragma unroll
-    for (int s = 0; s < MT::NS; ++s) w->zn[1][lane + 32 * s] = S.h * f[s];
+    for (int s = 0; s < MT::NS; ++s) w->zn[1][lane + MT::G * s] = S.h * f[s];
     return cv::TRY_AGAIN;
 }
 
@@ -496,7 +497,7 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
 #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
-        for (int s = 0; s < NS; ++s) w->zn[j][lane + 32 * s] = (j == 0 && valid_el<NS>(lane, s, N)) ? y0.v[s] : 0.0;
+        for (int s = 0; s < NS; ++s) w->zn[j][lane + MT::G * s] = (j == 0 && valid_el<MT::G>(lane, s, N)) ? y0.v[s] : 0.0;
     #pragma unroll 1
     for (int j = 0; j < 8; ++j) S.l[j] = S.tq[j] = S.tau[j] = 0.0;
     #pragma unroll 1
@@ -512,12 +513,12 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
     double ewt[NS], z0[NS], z1[NS], y[NS], tmp[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        z0[s] = valid_el<NS>(lane, s, N) ? y0.v[s] : 0.0;
-        ewt[s] = valid_el<NS>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(z0[s]) + S.atol) : 0.0;
+        z0[s] = valid_el<MT::G>(lane, s, N) ? y0.v[s] : 0.0;
+        ewt[s] = valid_el<MT::G>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(z0[s]) + S.atol) : 0.0;
     }
     bdf_rhs<MT, LinT>(off, z0, z1, lane);
 #pragma unroll
-    for (int s = 0; s < NS; ++s) if (!valid_el<NS>(lane, s, N)) z1[s] = 0.0;
+    for (int s = 0; s < NS; ++s) if (!valid_el<MT::G>(lane, s, N)) z1[s] = 0.0;
     // ---- cvHin
     const double tdiff = tout - t0;
     if (tdiff == 0.0) return cv::CV_TOO_CLOSE;
@@ -529,11 +530,11 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
     double r = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s)
-        if (valid_el<NS>(lane, s, N)) {
+        if (valid_el<MT::G>(lane, s, N)) {
             const double den = cv::HUB_FACTOR * fabs(z0[s]) + ode_div(1.0, ewt[s]);
             r = fmax(r, ode_div(fabs(z1[s]), den));
         }
-    const double hub_inv = warp_max(r);
+    const double hub_inv = group_max<MT::G>(r);
     double hub = cv::HUB_FACTOR * tdist;
     if (hub * hub_inv > 1.0) hub = ode_div(1.0, hub_inv);
     double hg = sqrt(hlb * hub);
@@ -551,7 +552,7 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
             const double ih = ode_div(1.0, hgs);
 #pragma unroll
             for (int s = 0; s < NS; ++s) tmp[s] = (tmp[s] - z1[s]) * ih;
-            const double yddnrm = wrms_v<NS>(tmp, ewt, N);
+            const double yddnrm = wrms_v<NS, MT::G>(tmp, ewt, N);
             hnew = (yddnrm * hub * hub > 2.0) ? sqrt(ode_div(2.0, yddnrm)) : sqrt(hg * hub);
             if (count1 == cv::MAX_HIN_ITERS) break;
             const double hrat = ode_div(hnew, hg);
@@ -568,7 +569,7 @@ __device__ __noinline__ int bdf_begin(unsigned off, const Vec<MT::NS> y0, double
     S.hscale = h0;
     S.hprime = h0;
 #pragma unroll
-    for (int s = 0; s < NS; ++s) w->zn[1][lane + 32 * s] = z1[s] * h0;
+    for (int s = 0; s < NS; ++s) w->zn[1][lane + MT::G * s] = z1[s] * h0;
     return 0;
 }
 
@@ -582,14 +583,14 @@ __device__ __noinline__ Vec<MT::NS> bdf_finish(unsigned off, int status, double 
     if (status == 0) {
         const double s_ = ode_div(tout - S.tn, S.h);
 #pragma unroll
-        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[S.q][lane + 32 * s];
+        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[S.q][lane + MT::G * s];
         #pragma unroll 1
         for (int j = S.q - 1; j >= 0; --j)
 #pragma unroll
-            for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[j][lane + 32 * s] + s_ * out.v[s];
+            for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[j][lane + MT::G * s] + s_ * out.v[s];
     } else {
 #pragma unroll
-        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[0][lane + 32 * s];
+        for (int s = 0; s < MT::NS; ++s) out.v[s] = w->zn[0][lane + MT::G * s];
     }
     S.cnt[C_NST] = S.nst;
     return out;
@@ -611,7 +612,7 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
         // ---- CVode loop: error weights, work limit, accuracy check
 #pragma unroll
         for (int s = 0; s < NS; ++s)
-            ewt[s] = valid_el<NS>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(w->zn[0][lane + 32 * s]) + S.atol) : 0.0;
+            ewt[s] = valid_el<MT::G>(lane, s, N) ? ode_div(1.0, S.rtol * fabs(w->zn[0][lane + MT::G * s]) + S.atol) : 0.0;
         if (S.nstloc >= S.max_steps) { done = true; return cv::CV_TOO_MUCH_WORK; }
         if (cv::UROUND * wrms_zn<MT, LinT>(w, 0, ewt, lane) > 1.0) { done = true; return cv::CV_TOO_MUCH_ACC; }
         // ---- cvStep
@@ -644,10 +645,10 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
             for (int attempt = 0; attempt < 4; ++attempt) {
                 // residual at ycor = acor
 #pragma unroll
-                for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + 32 * s] + acor[s];
+                for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + MT::G * s] + acor[s];
                 bdf_rhs<MT, LinT>(off, y, ftemp, lane);
 #pragma unroll
-                for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + 32 * s] + acor[s]);
+                for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + MT::G * s] + acor[s]);
                 if (call_setup) {
                     Vec<NS> yv;
 #pragma unroll
@@ -666,11 +667,11 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
                     bdf_solve<MT, LinT>(off, delta, wg, lane);
 #pragma unroll
                     for (int s = 0; s < NS; ++s) acor[s] += delta[s];
-                    const double del = wrms_v<NS>(delta, ewt, N);
+                    const double del = wrms_v<NS, MT::G>(delta, ewt, N);
                     if (m > 0) S.crate = fmax(cv::CRDOWN * S.crate, ode_div(del, delp));
                     const double dcon = ode_div(del * fmin(1.0, S.crate), S.tq[4]);
                     if (dcon <= 1.0) {
-                        S.acnrm = (m == 0) ? del : wrms_v<NS>(acor, ewt, N);
+                        S.acnrm = (m == 0) ? del : wrms_v<NS, MT::G>(acor, ewt, N);
                         S.jcur = 0;
                         converged = true;
                         break;
@@ -679,10 +680,10 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
                     delp = del;
                     if (m + 1 >= cv::NLS_MAXCOR) { ret = cv::CONV_RECVR; break; }
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + 32 * s] + acor[s];
+                    for (int s = 0; s < NS; ++s) y[s] = w->zn[0][lane + MT::G * s] + acor[s];
                     bdf_rhs<MT, LinT>(off, y, ftemp, lane);
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + 32 * s] + acor[s]);
+                    for (int s = 0; s < NS; ++s) delta[s] = -S.gamma * ftemp[s] + (S.rl1 * w->zn[1][lane + MT::G * s] + acor[s]);
                 }
                 if (converged) { ret = 0; break; }
                 if (ret == cv::CONV_RECVR && !S.jcur) {
@@ -731,12 +732,12 @@ __device__ __forceinline__ int bdf_advance(unsigned off, WarpGlobal<MT, LinT>* w
                 for (int j = 0; j <= q; ++j) {
                     const double lj = S.l[j];
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) w->zn[j][lane + 32 * s] += lj * acor[s];
+                    for (int s = 0; s < NS; ++s) w->zn[j][lane + MT::G * s] += lj * acor[s];
                 }
                 S.qwait--;
                 if (S.qwait == 1 && q != S.qmax) {
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + 32 * s] = acor[s];
+                    for (int s = 0; s < NS; ++s) w->zn[S.qmax][lane + MT::G * s] = acor[s];
                     S.saved_tq5 = S.tq[5];
                     S.indx_acor = S.qmax;
                 }
@@ -780,25 +781,25 @@ __device__ __noinline__ void bdf_save(unsigned off, unsigned char* rec, int phas
     const int* src = reinterpret_cast<const int*>(&w->st);
     int* dst = reinterpret_cast<int*>(rec);
 #pragma unroll 1
-    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
+    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += MT::G) dst[e] = src[e];
     if (lane == 0) *reinterpret_cast<int*>(rec + R::kPhaseOff) = phase;
     double* Z = reinterpret_cast<double*>(rec + R::kStateBytes + 8);
     #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s)
-            if (valid_el<MT::NS>(lane, s, N)) Z[j * N + lane + 32 * s] = w->zn[j][lane + 32 * s];
+            if (valid_el<MT::G>(lane, s, N)) Z[j * N + lane + MT::G * s] = w->zn[j][lane + MT::G * s];
     if (w->st.lu_dirty) {
         LinT* Ag = reinterpret_cast<LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
-        for (int e = lane; e < N * MT::LDA; e += 32) Ag[e] = w->A[e];
+        for (int e = lane; e < N * MT::LDA; e += MT::G) Ag[e] = w->A[e];
         #pragma unroll 1
-        for (int e = lane; e < N; e += 32) Ag[N * MT::LDA + e] = w->dinv[e];
+        for (int e = lane; e < N; e += MT::G) Ag[N * MT::LDA + e] = w->dinv[e];
         int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA + N);
         #pragma unroll 1
-        for (int e = lane; e < N; e += 32) pg[e] = w->perm[e];
+        for (int e = lane; e < N; e += MT::G) pg[e] = w->perm[e];
     }
-    __syncwarp();
+    __syncwarp(gmask<MT::G>());
 }
 
 template <class MT, class LinT>
@@ -809,22 +810,22 @@ __device__ __noinline__ void bdf_load(unsigned off, const unsigned char* rec, in
     const int* src = reinterpret_cast<const int*>(rec);
     int* dst = reinterpret_cast<int*>(&w->st);
 #pragma unroll 1
-    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += 32) dst[e] = src[e];
+    for (int e = lane; e < (int)(sizeof(BdfState) / 4); e += MT::G) dst[e] = src[e];
     const double* Z = reinterpret_cast<const double*>(rec + R::kStateBytes + 8);
     #pragma unroll 1
     for (int j = 0; j <= cv::QMAX; ++j)
 #pragma unroll
         for (int s = 0; s < MT::NS; ++s)
-            w->zn[j][lane + 32 * s] = valid_el<MT::NS>(lane, s, N) ? Z[j * N + lane + 32 * s] : 0.0;
+            w->zn[j][lane + MT::G * s] = valid_el<MT::G>(lane, s, N) ? Z[j * N + lane + MT::G * s] : 0.0;
     const LinT* Ag = reinterpret_cast<const LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
-    for (int e = lane; e < N * MT::LDA; e += 32) w->A[e] = Ag[e];
+    for (int e = lane; e < N * MT::LDA; e += MT::G) w->A[e] = Ag[e];
     #pragma unroll 1
-    for (int e = lane; e < N; e += 32) w->dinv[e] = Ag[N * MT::LDA + e];
+    for (int e = lane; e < N; e += MT::G) w->dinv[e] = Ag[N * MT::LDA + e];
     const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA + N);
     #pragma unroll 1
-    for (int e = lane; e < N; e += 32) w->perm[e] = pg[e];
-    __syncwarp();
+    for (int e = lane; e < N; e += MT::G) w->perm[e] = pg[e];
+    __syncwarp(gmask<MT::G>());
 }
 
 }  // namespace b200

@@ -1,14 +1,15 @@
 // Warp-per-cell chemistry: constant-pressure RHS and analytic Jacobian.
 //
-// One warp evaluates one cell.  The 32 lanes split the work three ways:
-//   * species phase   -- lane l owns species l and l+32 (thermo, concentrations);
-//   * reaction phase  -- lane l evaluates reaction slot 32*g + l of group g
+// One group of G lanes evaluates one cell (G = 32, a whole warp, except for the
+// smallest mechanisms; see MechT).  The lanes split the work three ways:
+//   * species phase   -- lane l owns species l, l+G, ... (thermo, concentrations);
+//   * reaction phase  -- lane l evaluates reaction slot G*g + l of group g
 //                        (kf, Kc, third-body / falloff modifiers, rates of progress);
 //   * gather phase    -- production rates summed from the rates of progress with
-//                        a balanced, coalesced (species, reaction) list: every lane
-//                        sums ~1/32 of the pairs in a fixed order, partial sums
-//                        are combined per species in a fixed order (no atomics,
-//                        so results do not depend on scheduling).
+//                        a balanced, coalesced (species, reaction) list dealt to
+//                        32 lists (lane l sums lists l, l+G, ...) in a fixed order;
+//                        partial sums are combined per species in a fixed order
+//                        (no atomics, so results do not depend on scheduling).
 // Per-cell intermediates (concentrations, -g/RT, rates) live in shared memory,
 // never in HBM (the reference's GPU path keeps ~31.8 KB of them per cell in global
 // memory: src/Mechanism/GPU/gpu_memory.cu:3-37).
@@ -39,14 +40,21 @@ constexpr double kRU = 8314.4621;
 // reaction code is on the instruction-fetch-bound hot path), and the reactor
 // formulation: constant pressure, or constant volume (CONV_ = 1; the kernels'
 // pressure slot then carries the cell's fixed density).  Both are compile-time
-// so a kernel holds no code of the other case.
-template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_, int CONV_ = 0>
+// so a kernel holds no code of the other case.  G_ is the number of lanes that
+// integrate one cell: 32 (a warp per cell), or 16 / 8 for the smallest
+// mechanisms, whose 9-10 species leave most of a warp idle in every vector
+// phase; then 2 or 4 cells share a warp, each on its aligned group of G lanes
+// (shuffles, votes and syncs take the group's mask), and the scalar step logic
+// every lane of a group repeats is issued once for all cells of the warp.
+template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_, int CONV_ = 0, int G_ = 32>
 struct MechT {
+    static_assert(G_ == 32 || G_ == 16 || G_ == 8, "lanes per cell: 32, 16 or 8");
     static constexpr int ID = ID_;                            // index into c_mech
     static constexpr int N = N_;                              // state length == species count
-    static constexpr int NS = (N_ + 31) / 32;                 // elements per lane
+    static constexpr int G = G_;                              // lanes per cell (32 / G cells per warp)
+    static constexpr int NS = (N_ + G_ - 1) / G_;             // elements per lane
     static constexpr int NSLOT = ((NR_ + 32) / 32) * 32;      // reaction slots (>= 1 padding slot)
-    static constexpr int NG = NSLOT / 32;                     // reaction groups
+    static constexpr int NG = NSLOT / G_;                     // reaction groups (G slots each)
     static constexpr int LDA = (N_ % 2 == 0) ? N_ + 1 : N_;   // odd stride: conflict-free rows/cols
     static constexpr int NU_DEN = NU_DEN_;                    // gather words hold nu * NU_DEN
     static constexpr int NUNITMAX = NUNITS_;                  // gather units (checked at creation)
@@ -61,7 +69,8 @@ __constant__ DevMech c_mech[kNumMech];
 template <class MT>
 __device__ __forceinline__ const DevMech& mech() { return c_mech[MT::ID]; }
 
-// A lane's slice of a state vector (element i = lane + 32*s), passed by value
+// A lane's slice of a state vector (element i = lane + G*s, lane within the
+// cell's group of MT::G lanes), passed by value
 // so the heavy phases can be single-copy (non-inlined) functions without
 // forcing the caller's state into local memory.
 template <int NS>
@@ -99,16 +108,35 @@ __device__ __forceinline__ T* smem_at(unsigned off) {
     return reinterpret_cast<T*>(dyn_smem() + off);
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
+// Mask of the aligned group of G lanes this thread belongs to.
+template <int G>
+__device__ __forceinline__ unsigned gmask() {
+    if constexpr (G == 32) return kFull;
+    else return ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+}
+
+// Sum / max over the thread's group of G lanes (every lane gets the result).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+    const unsigned m = gmask<G>();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(m, v, o, G);
     return v;
 }
-__device__ __forceinline__ double warp_max(double v) {
+template <int G>
+__device__ __forceinline__ double group_max(double v) {
+    const unsigned m = gmask<G>();
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(kFull, v, o));
+    for (int o = G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(m, v, o, G));
     return v;
 }
+// Value of lane `src` (0..G-1) of the thread's group.
+template <int G, class T>
+__device__ __forceinline__ T group_shfl(T v, int src) {
+    return __shfl_sync(gmask<G>(), v, src, G);
+}
+__device__ __forceinline__ double warp_sum(double v) { return group_sum<32>(v); }
+__device__ __forceinline__ double warp_max(double v) { return group_max<32>(v); }
 
 // Per-warp shared scratch of the chemistry.
 template <class MT>
@@ -164,24 +192,24 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
                                                     ChemSmem<MT>* sm, int lane, double (&Yk)[MT::NS],
                                                     double (&cpR)[MT::NS], double (&hRT)[MT::NS],
                                                     double (&dcpR)[MT::NS]) {
-    constexpr int N = MT::N;
+    constexpr int N = MT::N, G = MT::G;
     CellThermo c;
-    c.T = __shfl_sync(kFull, y[(N - 1) / 32], (N - 1) % 32);
+    c.T = group_shfl<G>(y[(N - 1) / G], (N - 1) % G);
     double sy = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         if (i < N - 1) sy += y[s];
     }
-    c.yN = 1.0 - warp_sum(sy);
+    c.yN = 1.0 - group_sum<G>(sy);
     double sw = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         Yk[s] = (i < N - 1) ? y[s] : ((i == N - 1) ? c.yN : 0.0);
         if (i < N) sw += Yk[s] * __ldg(M.inv_mw + i);
     }
-    c.mw_avg = ode_div(1.0, warp_sum(sw));
+    c.mw_avg = ode_div(1.0, group_sum<G>(sw));
     c.logT = log(c.T);
     c.invT = ode_div(1.0, c.T);
     if constexpr (!MT::CONV) {
@@ -196,7 +224,7 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     double csum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         if (i < N) {
             double g;
             nasa7(M, i, c.T, c.logT, c.invT, cpR[s], hRT[s], g, dcpR[s]);
@@ -209,13 +237,13 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
             cpR[s] = hRT[s] = dcpR[s] = 0.0;
         }
     }
-    c.mC = c.m - warp_sum(csum);
+    c.mC = c.m - group_sum<G>(csum);
     if (lane == 0) {
         sm->C[N] = 1.0;
         sm->G[N] = 0.0;
         sm->H[N] = 0.0;
     }
-    __syncwarp();
+    __syncwarp(gmask<G>());
     return c;
 }
 
@@ -416,14 +444,28 @@ __device__ __forceinline__ RxnCtx rxn_ctx(const CellThermo& c) { return RxnCtx{c
 // with the same operations a single warp would use, so results do not depend
 // on whether helpers serve.  The hand-off goes through a shared-memory control
 // block with bounded polling waits (no hardware barrier a warp could miss).
+//
+// Recovery when a wait runs out:
+//   * warp 0's wait for a command's completion (join) runs out: warp 0 keeps
+//     waiting, bounded again (drain), for the late shares.  If they arrive, the
+//     command's outputs are complete and the cell goes on unchanged; the helpers
+//     are released (kCmdExit) and warp 0 works alone for the rest of the launch.
+//   * the drain runs out too: a late helper might still write into warp 0's
+//     shared memory at any time, so the CTA is poisoned: the current cell and
+//     every later cell the CTA claims fail with CV_ERR_FAILURE, later cells
+//     without being integrated (their state is left as given).
+//   * a helper's wait for the next command runs out (warp 0 silent for ~10 s):
+//     the helper leaves; warp 0's next join and drain then run out (poisoned).
 constexpr int kWideN = 192;
 constexpr int kHelperWarps = 3;
 enum { kCmdRhs = 1, kCmdLu = 2, kCmdExit = 3 };
-// A helper waits for the next command at most ~10 s (warp 0 works alone
-// between commands: Jacobian, step control); warp 0 waits for a command's
-// completion at most ~2 s (a share takes microseconds).
+// Default limits in SM clock cycles: a helper waits for the next command at
+// most ~10 s (warp 0 works alone between commands: Jacobian, step control);
+// warp 0 waits for a command's completion ~2 s, then ~2 s more for late shares
+// (a share takes microseconds).
 constexpr long long kHelperIdleCycles = 20000000000LL;
 constexpr long long kJoinCycles = 4000000000LL;
+constexpr long long kDrainCycles = 4000000000LL;
 
 struct HelperCtl {
     unsigned seq;      // commands posted
@@ -431,9 +473,12 @@ struct HelperCtl {
     unsigned posted;   // warp 0's count of commands posted
     int cmd;
     int nhelpers;      // kHelperWarps while the helpers serve, else 0
-    int err;           // a bounded wait ran out
+    int err;           // a bounded wait ran out (join or helper idle)
+    int poisoned;      // a drain ran out: late helper writes possible, fail every cell
+    int exit_posted;   // kCmdExit posted (helpers released)
     int k0, kend;      // kCmdLu: the LU panel
     unsigned A_off, C_off, G_off, q_off;
+    long long join_cycles, drain_cycles, idle_cycles;   // wait limits of this launch
     RxnCtx rc;         // kCmdRhs: the cell's reaction context
 };
 // One per CTA, in the kernels of the mechanisms that use it.
@@ -455,21 +500,36 @@ __device__ __forceinline__ void helpers_post(HelperCtl* h, int cmd, int lane) {
     __syncwarp();
 }
 
-// Warp 0: wait until the helpers have finished every posted command.  If the
-// wait runs out, the helpers are dropped (nhelpers = 0) and err is set.
-__device__ __forceinline__ void helpers_join(HelperCtl* h, int lane) {
-    const unsigned expected = kHelperWarps * h->posted;
+// Warp 0: wait, at most `limit` cycles, until the helpers have reported
+// `expected` completions.  Every lane returns the same answer.
+__device__ __forceinline__ bool helpers_wait_done(HelperCtl* h, unsigned expected, long long limit) {
     const long long t0 = clock64();
     bool ok = true;
     while (ld_volatile(&h->done) < expected) {
-        if (clock64() - t0 > kJoinCycles) { ok = false; break; }
+        if (clock64() - t0 > limit) { ok = false; break; }
     }
     __threadfence_block();
-    ok = __all_sync(kFull, ok);
-    if (!ok && lane == 0) {
+    return __all_sync(kFull, ok);
+}
+
+// Warp 0: wait until the helpers have finished every posted command.  If the
+// join runs out, the drain waits for the late shares: when they arrive the
+// outputs are complete and the helpers are released (warp 0 alone from here
+// on); when the drain runs out too the CTA is poisoned (see above).  Either
+// way nhelpers becomes 0 and err is set.
+__device__ __noinline__ void helpers_join(HelperCtl* h, int lane) {
+    const unsigned expected = kHelperWarps * h->posted;
+    if (helpers_wait_done(h, expected, h->join_cycles)) return;
+    const bool drained = helpers_wait_done(h, expected, h->drain_cycles);
+    if (lane == 0) {
         h->err = 1;
         h->nhelpers = 0;
+        if (!drained) h->poisoned = 1;
     }
+    __syncwarp();
+    // release the helpers (a late one leaves once it has finished its share)
+    helpers_post(h, kCmdExit, lane);
+    if (lane == 0) h->exit_posted = 1;
     __syncwarp();
 }
 
@@ -478,6 +538,7 @@ __device__ __forceinline__ void helpers_join(HelperCtl* h, int lane) {
 template <class MT>
 __device__ __forceinline__ void rhs_groups(const RxnCtx rc, unsigned C_off, unsigned G_off, unsigned q_off, int g0,
                                            int dg, int lane) {
+    static_assert(MT::G == 32, "helper warps serve one cell per warp");
     double* q = smem_at<double>(q_off);
 #pragma unroll 1
     for (int g = g0; g < MT::NG; g += dg) {
@@ -503,41 +564,44 @@ __device__ __forceinline__ void rhs_groups_forked(const RxnCtx rc, unsigned C_of
         h->q_off = q_off;
     }
     helpers_post(h, kCmdRhs, lane);
-    constexpr int dg = kHelperWarps + 1;
-    rhs_groups<MT>(rc, C_off, G_off, q_off, 0, dg, lane);
+    rhs_groups<MT>(rc, C_off, G_off, q_off, 0, kHelperWarps + 1, lane);
+    // after a drained join every share is complete; a poisoned CTA fails the cell
     helpers_join(h, lane);
-    if (h->err) {   // helpers dropped: their groups again on this warp (the same values)
-        for (int w = 1; w < dg; ++w) rhs_groups<MT>(rc, C_off, G_off, q_off, w, dg, lane);
-    }
 }
 
-// Balanced gather: out[s] = sum over species (lane + 32 s)'s (slot, nu) pairs of
+// Balanced gather: out[s] = sum over species (lane + G s)'s (slot, nu) pairs of
 // nu * src[slot]; src is the shared-memory array at byte offset src_off, or,
 // with kGlobal, the global array gsrc.  Unit partial sums go through the
 // chemistry scratch's part[].  Out of line: the RHS and the Jacobian share it.
 template <class MT, bool kGlobal>
 __device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off, unsigned chem_off, int lane) {
+    constexpr int G = MT::G, LISTS = 32 / G;   // the tables deal the units to 32 lists
     const DevMech& M = mech<MT>();
     const double* src = kGlobal ? gsrc : smem_at<double>(src_off);
     ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
-    double acc = 0.0;
+    double acc[LISTS];
+#pragma unroll
+    for (int r = 0; r < LISTS; ++r) acc[r] = 0.0;
     const int gmax = M.gmax;
     const int* gw = M.gword + lane;
 #pragma unroll 2
     for (int e = 0; e < gmax; ++e) {
-        const int w = __ldg(gw + 32 * e);
-        double nu = (double)(((w >> 11) & 31) - 16);
-        if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
-        acc += nu * src[w & 2047];
-        const bool last = (w >> 16) & 1;
-        if (last) sm->part[w >> 17] = acc;
-        acc = last ? 0.0 : acc;
+#pragma unroll
+        for (int r = 0; r < LISTS; ++r) {   // lane's lists: lane, lane + G, ...
+            const int w = __ldg(gw + 32 * e + G * r);
+            double nu = (double)(((w >> 11) & 31) - 16);
+            if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
+            acc[r] += nu * src[w & 2047];
+            const bool last = (w >> 16) & 1;
+            if (last) sm->part[w >> 17] = acc[r];
+            acc[r] = last ? 0.0 : acc[r];
+        }
     }
-    __syncwarp();
+    __syncwarp(gmask<G>());
     Vec<MT::NS> out;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         double v = 0.0;
         if (i < MT::N) {
             const int u0 = __ldg(M.unit_off + i), u1 = __ldg(M.unit_off + i + 1);
@@ -545,14 +609,14 @@ __device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off,
         }
         out.v[s] = v;
     }
-    __syncwarp();
+    __syncwarp(gmask<G>());
     return out;
 }
 
 // f = dy/dt for the warp's cell.  y, f: lane elements in internal order.
 template <class MT>
 __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, unsigned chem_off, int lane) {
-    constexpr int N = MT::N;
+    constexpr int N = MT::N, G = MT::G;
     const DevMech& M = mech<MT>();
     ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
     double y[MT::NS];
@@ -567,11 +631,11 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
     } else {
 #pragma unroll 1
         for (int g = 0; g < MT::NG; ++g) {
-            const int s = 32 * g + lane;
+            const int s = G * g + lane;
             sm->q[s] = rxn_slot<MT>(s, rc, C_off, G_off, 0).q;
         }
     }
-    __syncwarp();
+    __syncwarp(gmask<G>());
     double om[MT::NS];
     {
         const Vec<MT::NS> g = gather<MT, false>(nullptr, smem_off(sm->q), chem_off, lane);
@@ -583,7 +647,7 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
     double qsum = 0.0, cpsum = 0.0;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         if (i < N) {
             if constexpr (!MT::CONV) {
                 qsum += om[s] * hRT[s];
@@ -594,19 +658,19 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
             }
         }
     }
-    const double Q = kRU * c.T * warp_sum(qsum);          // sum_k w_k e_k W_k   [W/m^3]
-    const double cp_avg = kRU * warp_sum(cpsum);           // cp or cv [J/kg/K]
+    const double Q = kRU * c.T * group_sum<G>(qsum);      // sum_k w_k e_k W_k   [W/m^3]
+    const double cp_avg = kRU * group_sum<G>(cpsum);       // cp or cv [J/kg/K]
     const double dTdt = ode_div(-Q, c.rho * cp_avg);
     const double inv_rho = ode_div(1.0, c.rho);
     Vec<MT::NS> fv;
 #pragma unroll
     for (int s = 0; s < MT::NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         if (i < N - 1) fv.v[s] = om[s] * (__ldg(M.mw + i) * inv_rho);
         else if (i == N - 1) fv.v[s] = dTdt;
         else fv.v[s] = 0.0;
     }
-    __syncwarp();   // shared scratch is reused by the next evaluation
+    __syncwarp(gmask<G>());   // shared scratch is reused by the next evaluation
     return fv;
 }
 
@@ -622,7 +686,8 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 template <class MT, class LinT>
 __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A_off, unsigned chem_off,
                                       JacScratch<MT>* js, int lane) {
-    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
+    const unsigned gm = gmask<G>();
     const DevMech& M = mech<MT>();
     LinT* A = smem_at<LinT>(A_off);
     ChemSmem<MT>* sm = smem_at<ChemSmem<MT>>(chem_off);
@@ -631,7 +696,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     for (int s = 0; s < NS; ++s) y[s] = yv.v[s];
     double Yk[NS], cpR[NS], hRT[NS], dcpR[NS];
 #pragma unroll 2
-    for (int e = lane; e < N * LDA; e += 32) A[e] = LinT(0);
+    for (int e = lane; e < N * LDA; e += G) A[e] = LinT(0);
     const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
     constexpr bool conv = MT::CONV;   // constant volume (see species_phase)
     constexpr int ns = MT::NSLOT;
@@ -639,7 +704,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     const unsigned C_off = smem_off(sm->C), G_off = smem_off(sm->G);
 #pragma unroll 1
     for (int g = 0; g < MT::NG; ++g) {
-        const int s = 32 * g + lane;
+        const int s = G * g + lane;
         const RxnOut o = rxn_slot<MT>(s, rc, C_off, G_off, 1);
         const int fl = __ldg(M.flags + s);
         double dqdT = 0.0, sr = 0.0, thd_term = 0.0;
@@ -725,7 +790,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             }
         }
     }
-    __syncwarp();
+    __syncwarp(gm);
     // per-species totals (fixed-order gathers)
     const Vec<NS> wv = gather<MT, false>(nullptr, smem_off(sm->q), chem_off, lane);
     const Vec<NS> dwv = gather<MT, true>(js->dqdT, 0u, chem_off, lane);
@@ -741,7 +806,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     double qsum = 0.0, cpsum = 0.0, Ssum2 = 0.0, Ssum3 = 0.0, accTT = 0.0, dcpsum = 0.0;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         dfdT[s] = 0.0;
         if (i < N) {
             const double Wi = __ldg(M.mw + i), iWi = __ldg(M.inv_mw + i);
@@ -766,17 +831,17 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             dcpsum += Yk[s] * kRU * dcpR[s] * iWi;
         }
     }
-    const double inv_cp = ode_div(1.0, warp_sum(cpsum));
-    const double fT = -warp_sum(qsum) * inv_cp;
-    const double S2 = warp_sum(Ssum2);
-    const double S3 = warp_sum(Ssum3);
-    const double JTT = -(warp_sum(accTT) + fT * warp_sum(dcpsum)) * inv_cp;
-    __syncwarp();
+    const double inv_cp = ode_div(1.0, group_sum<G>(cpsum));
+    const double fT = -group_sum<G>(qsum) * inv_cp;
+    const double S2 = group_sum<G>(Ssum2);
+    const double S3 = group_sum<G>(Ssum3);
+    const double JTT = -(group_sum<G>(accTT) + fT * group_sum<G>(dcpsum)) * inv_cp;
+    __syncwarp(gm);
     // T row (state row N-1): lane owns columns j < N-1
     double trow[NS];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int j = lane + 32 * s;
+        const int j = lane + G * s;
         trow[s] = 0.0;
         if (j < N - 1) {
             double S1 = 0.0;
@@ -786,11 +851,11 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             trow[s] = -(S1 * iWj - S2 * iWN + (iWj - iWN) * S3 + fT * (spw[N + j] - spw[N + N - 1])) * inv_cp;
         }
     }
-    __syncwarp();
+    __syncwarp(gm);
     // species rows k < N-1 (lane owns rows), then the T column
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int k = lane + 32 * s;
+        const int k = lane + G * s;
         if (k < N - 1) {
             LinT* row = A + k * LDA;
             const double Wk = __ldg(M.mw + k);
@@ -806,11 +871,11 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     }
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int j = lane + 32 * s;
+        const int j = lane + G * s;
         if (j < N - 1) A[(N - 1) * LDA + j] = (LinT)trow[s];
     }
     if (lane == 0) A[(N - 1) * LDA + (N - 1)] = (LinT)JTT;
-    __syncwarp();
+    __syncwarp(gm);
 }
 
 }  // namespace b200

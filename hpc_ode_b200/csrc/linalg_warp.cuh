@@ -33,6 +33,7 @@ __device__ __forceinline__ T absT(T v) { return v < T(0) ? -v : v; }
 // warp updates it, so splitting the columns does not change the factors.
 template <class MT, class LinT>
 __device__ __forceinline__ void lu_trailing(LinT* A, int k0, int kend, int lane, int w, int nw) {
+    static_assert(MT::G == 32, "the blocked LU serves one cell per warp");
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
     constexpr int kPanel = 4;
     constexpr int kRows = sizeof(LinT) == 4 ? 8 : 4;
@@ -123,6 +124,7 @@ __device__ __forceinline__ void lu_trailing_forked(unsigned A_off, int k0, int k
 // else hides it).
 template <class MT, class LinT>
 __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+    static_assert(MT::G == 32, "the blocked LU serves one cell per warp");
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
     constexpr int kPanel = 4;                               // panel width
     constexpr int kRows = sizeof(LinT) == 4 ? 8 : 4;        // rows per trailing-update batch
@@ -250,60 +252,91 @@ __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off
 // form's larger code costs more than it saves.
 template <class MT, class LinT>
 __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
-    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
+    const unsigned gm = gmask<G>();
     LinT* A = smem_at<LinT>(A_off);
     int* perm = smem_at<int>(perm_off);
     LinT* dinv = smem_at<LinT>(dinv_off);
     int sing = 0;
-    int pv[NS];   // lane tracks perm[i] for i = lane + 32 s
+    int pv[NS];   // lane tracks perm[i] for i = lane + G s
 #pragma unroll
-    for (int s = 0; s < NS; ++s) pv[s] = lane + 32 * s;
+    for (int s = 0; s < NS; ++s) pv[s] = lane + G * s;
 #pragma unroll 1
     for (int k = 0; k < N; ++k) {
         LinT best = LinT(-1);
         int bi = N;
-        for (int i = k + lane; i < N; i += 32) {
+        for (int i = k + lane; i < N; i += G) {
             const LinT v = absT(A[i * LDA + k]);
             if (v > best) { best = v; bi = i; }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const LinT ov = __shfl_xor_sync(kFull, best, o);
-            const int oi = __shfl_xor_sync(kFull, bi, o);
+        for (int o = G / 2; o > 0; o >>= 1) {
+            const LinT ov = __shfl_xor_sync(gm, best, o, G);
+            const int oi = __shfl_xor_sync(gm, bi, o, G);
             if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
         }
         if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
         if (bi != k) {
 #pragma unroll 1
-            for (int j = lane; j < N; j += 32) {
+            for (int j = lane; j < N; j += G) {
                 const LinT t = A[k * LDA + j];
                 A[k * LDA + j] = A[bi * LDA + j];
                 A[bi * LDA + j] = t;
             }
-            const int ok = __shfl_sync(kFull, pick<NS>(pv, k >> 5), k & 31);
-            const int ob = __shfl_sync(kFull, pick<NS>(pv, bi >> 5), bi & 31);
-            if (lane == (k & 31)) place<NS>(pv, k >> 5, ob);
-            if (lane == (bi & 31)) place<NS>(pv, bi >> 5, ok);
-            __syncwarp();
+            const int ok = group_shfl<G>(pick<NS>(pv, k / G), k % G);
+            const int ob = group_shfl<G>(pick<NS>(pv, bi / G), bi % G);
+            if (lane == (k % G)) place<NS>(pv, k / G, ob);
+            if (lane == (bi % G)) place<NS>(pv, bi / G, ok);
+            __syncwarp(gm);
         }
         const LinT inv = LinT(1) / A[k * LDA + k];
         if (lane == 0) dinv[k] = inv;
-        for (int i = k + 1 + lane; i < N; i += 32) A[i * LDA + k] *= inv;
-        __syncwarp();
-        // rank-1 update of the trailing block; lane owns columns j
-        for (int j = k + 1 + lane; j < N; j += 32) {
-            const LinT ukj = A[k * LDA + j];
-            if (ukj != LinT(0)) {
-#pragma unroll 4
-                for (int i = k + 1; i < N; ++i) A[i * LDA + j] -= A[i * LDA + k] * ukj;
+        for (int i = k + 1 + lane; i < N; i += G) A[i * LDA + k] *= inv;
+        __syncwarp(gm);
+        // rank-1 update of the trailing block; lane owns columns j = lane + G s > k.
+        // Rows go in batches of kRows whose multipliers and entries are all
+        // loaded before any store (a load may not pass a store to the same
+        // array, so element-by-element updates would each wait out the full
+        // shared-memory latency); every element gets the same single fused
+        // multiply-add as in the element-by-element form.
+        constexpr int kRows = 8;
+        LinT u[NS];
+        bool on[NS];
+        bool any = false;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int j = lane + G * s;
+            u[s] = (j > k && j < N) ? A[k * LDA + j] : LinT(0);
+            on[s] = u[s] != LinT(0);
+            any = any || on[s];
+        }
+        if (__any_sync(gm, any)) {
+#pragma unroll 1
+            for (int i0 = k + 1; i0 < N; i0 += kRows) {
+                LinT l[kRows];
+#pragma unroll
+                for (int r = 0; r < kRows; ++r) l[r] = (i0 + r < N) ? A[(i0 + r) * LDA + k] : LinT(0);
+#pragma unroll
+                for (int s = 0; s < NS; ++s) {
+                    if (on[s]) {
+                        const int j = lane + G * s;
+                        LinT a[kRows];
+#pragma unroll
+                        for (int r = 0; r < kRows; ++r)
+                            if (i0 + r < N) a[r] = A[(i0 + r) * LDA + j];
+#pragma unroll
+                        for (int r = 0; r < kRows; ++r)
+                            if (i0 + r < N) A[(i0 + r) * LDA + j] = a[r] - l[r] * u[s];
+                    }
+                }
             }
         }
-        __syncwarp();
+        __syncwarp(gm);
     }
 #pragma unroll
     for (int s = 0; s < NS; ++s)
-        if (lane + 32 * s < N) perm[lane + 32 * s] = pv[s];
-    __syncwarp();
+        if (lane + G * s < N) perm[lane + G * s] = pv[s];
+    __syncwarp(gm);
     return sing;
 }
 
@@ -316,12 +349,12 @@ __device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned 
     else return warp_lu_compact<MT, LinT>(A_off, perm_off, dinv_off, lane);
 }
 
-// Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + 32 s) in,
+// Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + G s) in,
 // solution out.  Arithmetic in LinT.
 template <class MT, class LinT>
 __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_off, unsigned dinv_off,
                                                   const Vec<MT::NS> bv, int lane) {
-    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
+    constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
     const LinT* A = smem_at<LinT>(A_off);
     const int* perm = smem_at<int>(perm_off);
     const LinT* dinv = smem_at<LinT>(dinv_off);
@@ -331,13 +364,13 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
     // gather: x[i] = b[perm[i]]
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         const int src = (i < N) ? perm[i] : i;
         double v = 0.0;
 #pragma unroll
         for (int s2 = 0; s2 < NS; ++s2) {
-            const double t = __shfl_sync(kFull, b[s2], src & 31);
-            if ((src >> 5) == s2) v = t;
+            const double t = group_shfl<G>(b[s2], src % G);
+            if ((src / G) == s2) v = t;
         }
         x[s] = (i < N) ? (LinT)v : LinT(0);
     }
@@ -345,21 +378,21 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
     // stay small in the instruction cache)
 #pragma unroll 1
     for (int k = 0; k < N - 1; ++k) {
-        const LinT xk = __shfl_sync(kFull, pick<NS>(x, k >> 5), k & 31);
+        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            const int i = lane + 32 * s;
+            const int i = lane + G * s;
             if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
         }
     }
     // backward: upper
 #pragma unroll 1
     for (int k = N - 1; k >= 0; --k) {
-        const LinT xk = __shfl_sync(kFull, pick<NS>(x, k >> 5), k & 31) * dinv[k];
-        if (lane == (k & 31)) place<NS>(x, k >> 5, xk);
+        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dinv[k];
+        if (lane == (k % G)) place<NS>(x, k / G, xk);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
-            const int i = lane + 32 * s;
+            const int i = lane + G * s;
             if (i < k) x[s] -= A[i * LDA + k] * xk;
         }
     }
@@ -370,7 +403,7 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
     const DevMech& M = mech<MT>();
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
-        const int i = lane + 32 * s;
+        const int i = lane + G * s;
         out.v[s] = (i < N - 1 && __ldg(M.inert + i)) ? b[s] : (double)x[s];
     }
     return out;

@@ -30,7 +30,7 @@ EXPORTED = ["b200ode_default_options", "b200ode_create", "b200ode_destroy", "b20
             "b200ode_integrate", "b200ode_integrate_device", "b200ode_integrate_device_noalloc",
             "b200ode_eval_rhs",
             "b200ode_eval_jacobian", "b200ode_eval_enthalpy", "b200ode_eval_enthalpy_device",
-            "b200ode_autotune", "b200ode_fp64_peak",
+            "b200ode_autotune", "b200ode_get_options", "b200ode_fp64_peak", "b200ode_fp32_peak",
             "b200ode_default_server_options", "b200ode_server_create", "b200ode_server_destroy",
             "b200ode_submit", "b200ode_poll", "b200ode_server_get_report",
             "b200ode_last_error", "b200ode_version"]
@@ -52,7 +52,10 @@ class Options(C.Structure):
                 ("persistent", C.c_int32), ("warps_per_block", C.c_int32),
                 ("blocks_per_sm", C.c_int32), ("queue_chunk", C.c_int32),
                 ("use_graph", C.c_int32), ("device", C.c_int32), ("profile_phases", C.c_int32),
-                ("formulation", C.c_int32), ("cta_helpers", C.c_int32)]
+                ("formulation", C.c_int32), ("cta_helpers", C.c_int32),
+                ("helper_join_cycles", C.c_int64), ("helper_drain_cycles", C.c_int64),
+                ("helper_idle_cycles", C.c_int64), ("max_cells_per_launch", C.c_int64),
+                ("lanes_per_cell", C.c_int32)]
 
 
 _i32p = C.POINTER(C.c_int32)
@@ -133,6 +136,10 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.b200ode_autotune.restype = C.c_int
     lib.b200ode_fp64_peak.argtypes = [C.c_int32, C.POINTER(C.c_double)]
     lib.b200ode_fp64_peak.restype = C.c_int
+    lib.b200ode_fp32_peak.argtypes = [C.c_int32, C.POINTER(C.c_double)]
+    lib.b200ode_fp32_peak.restype = C.c_int
+    lib.b200ode_get_options.argtypes = [C.c_void_p, C.POINTER(Options)]
+    lib.b200ode_get_options.restype = C.c_int
     lib.b200ode_default_server_options.argtypes = [C.POINTER(ServerOptions)]
     lib.b200ode_default_server_options.restype = None
     lib.b200ode_server_create.argtypes = [C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]
@@ -272,8 +279,14 @@ class Solver:
         w, b = C.c_int32(), C.c_int32()
         _check(self.lib.b200ode_autotune(self.h, n, C.c_void_p(dP or None), float(P_scalar), C.c_void_p(dT),
                                          C.c_void_p(dY), float(t0), float(t1), C.byref(w), C.byref(b)))
-        self.opts.warps_per_block, self.opts.blocks_per_sm = w.value, b.value
+        self.opts = self.options()
         return w.value, b.value
+
+    def options(self) -> Options:
+        """The options the handle uses now (defaults resolved, autotuned choices)."""
+        o = Options()
+        _check(self.lib.b200ode_get_options(self.h, C.byref(o)))
+        return o
 
     def integrate_device_noalloc(self, n: int, dP: int, P_scalar: float, dT: int, dY: int, t1: float,
                                  t0: float = 0.0, dstatus: int = 0, stream: int = 0, want_stats=True):
@@ -358,6 +371,13 @@ def fp64_peak_gflops(device: int = -1) -> float:
     """Measured FP64 FMA throughput of the device (GFLOP/s)."""
     g = C.c_double()
     _check(load().b200ode_fp64_peak(int(device), C.byref(g)))
+    return g.value
+
+
+def fp32_peak_gflops(device: int = -1) -> float:
+    """Measured FP32 FMA throughput of the device (GFLOP/s)."""
+    g = C.c_double()
+    _check(load().b200ode_fp32_peak(int(device), C.byref(g)))
     return g.value
 
 

@@ -61,3 +61,16 @@ def algorithmic_flops(mech: str, totals: Dict[str, float]) -> float:
             + totals["total_nsetups"] * (c["F_M"] + c["F_lu"])
             + totals["total_nni"] * c["F_solve"]
             + totals["total_nst"] * c["F_step"])
+
+
+def flops_by_pipe(mech: str, totals: Dict[str, float], mixed: bool):
+    """(FP64 flops, FP32 flops) of one batch from total counters.  In the mixed
+    form the Newton matrix M = I - gamma J, its LU and the triangular solves run
+    in FP32; the RHS, the Jacobian's chain rule (accumulated into the FP32
+    matrix) and the step logic stay FP64.  In the FP64 form all of it is FP64."""
+    c = op_counts(mech)
+    f64 = (totals["total_nfe"] * (c["F_rhs"] + c["T_rhs"])
+           + totals["total_nje"] * (c["F_jac"] + c["T_jac"])
+           + totals["total_nst"] * c["F_step"])
+    lin = totals["total_nsetups"] * (c["F_M"] + c["F_lu"]) + totals["total_nni"] * c["F_solve"]
+    return (f64, lin) if mixed else (f64 + lin, 0.0)

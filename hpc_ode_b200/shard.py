@@ -53,6 +53,14 @@ def balanced_ranges(cost: Sequence[float], world: int) -> List[Tuple[int, int]]:
     return [(bounds[r], bounds[r + 1]) for r in range(world)]
 
 
+def rank_range(T: np.ndarray, world: int, rank: int, cost: Optional[np.ndarray] = None) -> Tuple[int, int]:
+    """This rank's [start, stop) of a batch every rank holds identically, from
+    the batch's own data alone (no communication): cost-balanced contiguous
+    ranges by the temperature proxy, or by `cost` when given."""
+    ranges = balanced_ranges(temperature_cost(T) if cost is None else cost, world)
+    return ranges[rank]
+
+
 def shard_of(ranges: List[Tuple[int, int]], rank: int) -> slice:
     a, b = ranges[rank]
     return slice(a, b)
@@ -67,8 +75,7 @@ def integrate_shard(rank: int, world: int, T: np.ndarray, Y: np.ndarray, P, dt: 
     P_part, dt)` advances a contiguous part in place and returns its per-cell
     status.  Returns (slice, T_part, Y_part, status_part)."""
     n = T.size
-    ranges = balanced_ranges(temperature_cost(T) if cost is None else cost, world)
-    sl = shard_of(ranges, rank)
+    sl = slice(*rank_range(T, world, rank, cost))
     Tp = np.ascontiguousarray(T[sl].copy())
     Yp = np.ascontiguousarray(Y[:, sl].copy())
     Pp = P if np.ndim(P) == 0 else np.ascontiguousarray(np.asarray(P)[sl])

@@ -88,6 +88,26 @@ typedef struct {
                                  1 (default) = the CTA's other three warps take shares of the
                                  cell's reaction groups and LU updates; 0 = one warp per cell.
                                  Results are the same either way. */
+    /* Wait limits of that hand-off in SM clock cycles (0 = defaults: join ~2 s, drain ~2 s,
+       helper idle ~10 s).  Diagnostics for the recovery paths: when warp 0's wait for a
+       share (join) runs out it waits once more (drain); late shares that arrive then leave
+       the cell's results unchanged and warp 0 goes on alone; if the drain runs out too,
+       the CTA fails its current cell and every later cell it claims with
+       B200ODE_CELL_ERR_FAILURE (later ones left as given). */
+    int64_t helper_join_cycles;
+    int64_t helper_drain_cycles;
+    int64_t helper_idle_cycles;
+    /* Largest number of cells one launch sequence takes (0 = as many as fit: 80 % of the
+       free device memory over the per-cell footprint, as the reference's calc_gpu_points
+       sizes its batches).  A larger call runs as consecutive launches over contiguous
+       chunks of cells; results do not depend on the chunking. */
+    int64_t max_cells_per_launch;
+    /* Lanes of a warp that integrate one cell (0 = the mechanism's default): 32 (one cell per
+       warp) for every mechanism; the H2 mechanisms (h2o2, h2_li_2004: 9-10 unknowns) also
+       take 16 or 8 (2 or 4 cells per warp), which the autotuner may pick.  The right-hand
+       side is bitwise the same for every choice; the Jacobian's shared-memory accumulation
+       order is not, so results agree to within the integration tolerances, not bitwise. */
+    int32_t lanes_per_cell;
 } b200ode_options;
 
 /* Optional per-cell counters (CVodeGetNum* equivalents) and call totals.  Any
@@ -170,11 +190,16 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, cons
  * library keeps until the process exits.
  *
  *  - Always runs the persistent kernel (options.persistent and use_graph are
- *    not used).  A launch needs 256 bytes + resident warps x per-warp scratch
- *    (16.9 KB for GRI-Mech 3.0 in mixed precision, 28.1 KB in FP64); one that
- *    needs more than the array is refused with B200ODE_ERR_INVALID and the
- *    numbers in b200ode_last_error().  On a 148-SM B200 every launch shape the
- *    options allow fits; the number of cells is not limited.
+ *    not used), with the launch shape b200ode_integrate_device would use.  A
+ *    launch needs 256 bytes + resident cells x per-cell scratch (16.9 KB for
+ *    GRI-Mech 3.0 in mixed precision, 28.1 KB in FP64); one that needs more than
+ *    the array is refused with B200ODE_ERR_INVALID and the numbers in
+ *    b200ode_last_error().  On a 148-SM B200 the default launches of GRI-Mech
+ *    3.0 and the H2 mechanisms (either precision) and of n-dodecane in mixed
+ *    precision fit; n-dodecane in FP64 (about 89 KB per cell, two cells per SM)
+ *    fits only with options.blocks_per_sm = 1, and the 214-species kerosene
+ *    mechanism (208 KB per cell) does not fit.  The number of cells is not
+ *    limited.
  *  - The first call on a device looks up the array's device address there (and,
  *    with lazy module loading, is when the driver loads this library's kernels
  *    onto that device).  Make that first call before any stream capture.
@@ -220,21 +245,36 @@ b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n_cells, 
                                             const double* d_Y, double* d_h_mass, void* stream);
 
 /* Autotuner: integrates a sample of the given cells (the first min(n_cells,
- * 8192); device buffers as b200ode_integrate_device, left unmodified) with the
- * persistent kernel under each launch shape -- 4, 2 or 1 warps (cells) per CTA,
- * each with the full-register or the 168-register kernel variant -- and keeps
- * the fastest in the handle's options (warps_per_block, blocks_per_sm), which
- * later calls on this handle use.  The chosen values are also returned (either
- * pointer may be NULL).  Results of an integration do not depend on the launch
- * shape.  No reference counterpart (the reference has no tunable kernels). */
+ * 8192), or two per SM for the 214-species mechanism; device buffers as
+ * b200ode_integrate_device, left unmodified) with the persistent kernel and
+ * keeps the fastest choice in the handle's options, which later calls on this
+ * handle use.  Stage 1 times every launch shape: threads per cell (a warp, or
+ * for the H2 mechanisms 16 or 8 lanes -- 2 or 4 cells per warp; for the
+ * 214-species mechanism one 4-warp CTA per cell or one warp) x 4, 2 or 1 warps
+ * per CTA x the full-register or the 168-register kernel variant, skipping
+ * shapes whose shared memory exceeds a CTA's; stage 2 times the work-queue
+ * chunk (1, 2 or 8 cells per claim) on the chosen shape.  The chosen
+ * warps_per_block and blocks_per_sm are also returned (either pointer may be
+ * NULL); b200ode_get_options returns all of them (lanes_per_cell, cta_helpers,
+ * queue_chunk).  No reference counterpart: MAGMA's batched LU picks its kernel
+ * by a fixed size crossover (ext/magma-2.6.2/control/get_batched_crossover.cpp). */
 b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n_cells, const double* d_P, double P_scalar,
                                 const double* d_T, const double* d_Y, double t0, double t1,
                                 int32_t* warps_per_block, int32_t* blocks_per_sm);
+
+/* The options a handle uses now (after creation defaults were resolved and any
+ * autotuning).  No reference counterpart. */
+b200ode_status b200ode_get_options(const b200ode_handle* h, b200ode_options* out);
 
 /* Diagnostic: measured FP64 FMA throughput of a device (GFLOP/s), the
  * denominator of the FP64-pipe roofline this library reports.  No reference
  * counterpart (a measurement helper). */
 b200ode_status b200ode_fp64_peak(int32_t device, double* gflops);
+
+/* Diagnostic: measured FP32 FMA throughput of a device (GFLOP/s), the
+ * denominator of the FP32 part of the roofline (the mixed form's Newton matrix,
+ * LU and solves).  No reference counterpart (a measurement helper). */
+b200ode_status b200ode_fp32_peak(int32_t device, double* gflops);
 
 /* ------------------------------------------------------------------ serving
  * A request loop for an operator-split flow solver that sends chemistry batches

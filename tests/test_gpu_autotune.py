@@ -1,6 +1,9 @@
-"""The launch-shape autotuner (b200ode_autotune): it leaves the sample cells
-untouched, picks one of its candidate shapes, and integration results do not
-depend on the launch shape (bitwise)."""
+"""The autotuner (b200ode_autotune): it leaves the sample cells untouched,
+picks one of its candidates (threads per cell, warps per CTA, register variant,
+helper warps, work-queue chunk), and integration results do not depend on the
+launch shape (bitwise for one warp per cell; within the parity gates when the
+H2 mechanisms put several cells in a warp, whose Jacobian accumulates in another
+order)."""
 import numpy as np
 import pytest
 
@@ -21,6 +24,9 @@ def test_autotune_picks_a_shape_and_results_do_not_change(precision):
     wpb, bps = s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
     torch.cuda.synchronize()
     assert (wpb, bps) in {(4, 0), (2, 0), (1, 0), (4, 3), (2, 6), (1, 12)}
+    o = s.options()
+    assert o.lanes_per_cell == 32 and o.queue_chunk in (1, 2, 8)
+    assert (o.warps_per_block, o.blocks_per_sm) == (wpb, bps)
     assert torch.equal(T, T0) and torch.equal(Y, Y0)          # sample left untouched
     st = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
     s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt, dstatus=st.data_ptr())
@@ -48,6 +54,7 @@ def test_autotune_skips_shapes_that_do_not_fit():
     wpb, bps = s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
     torch.cuda.synchronize()
     assert wpb == 1 and bps in (0, 12)
+    assert s.options().cta_helpers in (0, 1)
     assert torch.equal(T, T0) and torch.equal(Y, Y0)
     s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
     s.close()
@@ -57,3 +64,31 @@ def test_autotune_skips_shapes_that_do_not_fit():
     ref.close()
     torch.cuda.synchronize()
     assert torch.equal(T, T2) and torch.equal(Y, Y2)
+
+
+def test_autotune_h2_tries_several_cells_per_warp(oracle):
+    """The 10-species H2 mechanism: threads per cell 32, 16 or 8 (1, 2 or 4 cells
+    per warp) are candidates; whichever is kept, the integration passes the
+    parity gates against the CPU oracle."""
+    import torch
+    b = W.make("h2_1024", 4096, seed=19)
+    T = torch.from_numpy(b.T.copy()).cuda()
+    Y = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
+    P = torch.from_numpy(b.P.copy()).cuda()
+    s = native.Solver(b.mech)
+    s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
+    o = s.options()
+    assert o.lanes_per_cell in (32, 16, 8) and o.queue_chunk in (1, 2, 8)
+    st = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
+    s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt, dstatus=st.data_ptr())
+    s.close()
+    torch.cuda.synchronize()
+    assert (st == 0).all()
+    idx = np.arange(0, b.ncells, 16)
+    sub = b.subset(idx)
+    yo, so = oracle.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, threads=8)
+    Tg = T.cpu().numpy()[idx]
+    Yg = Y.cpu().numpy()[:-1, idx].T
+    assert (np.abs(Tg - yo[:, 0]) / yo[:, 0]).max() <= 1e-5
+    ok = np.abs(Yg - yo[:, 1:]) <= np.maximum(1e-4 * np.abs(yo[:, 1:]), 1e-10)
+    assert ok.mean() >= 0.99

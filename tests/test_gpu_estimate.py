@@ -129,3 +129,47 @@ def test_helper_warps_do_not_change_results(persistent):
     assert (out[0][2] == 0).all()
     for a, c in zip(out[0], out[1]):
         assert np.array_equal(a, c)
+
+
+def _helper_run(b, **kw):
+    s = native.Solver(MECH, **kw)
+    T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+    st, stats, cnt = s.integrate(T, Y, b.P, b.dt, counters=True)
+    s.close()
+    return T, Y, st, cnt["nst"]
+
+
+def test_helper_join_timeout_keeps_results():
+    """Warp 0's wait for its helpers' shares (join) limited to one clock cycle:
+    when it runs out, warp 0 waits again (drain, default limit) until the late
+    shares are in, releases the helpers and goes on alone.  Every share still
+    completes before warp 0 reads it, so results, statuses and step counts equal
+    the one-warp launch bitwise."""
+    b = _cells(24, seed=9)
+    ref = _helper_run(b, cta_helpers=0)
+    got = _helper_run(b, cta_helpers=1, helper_join_cycles=1)
+    assert (ref[2] == 0).all()
+    for a, c in zip(got, ref):
+        assert np.array_equal(a, c)
+
+
+def test_helper_drain_timeout_fails_cells_and_returns():
+    """All hand-off waits limited to a few hundred cycles: the helpers leave
+    while warp 0 works alone between commands, so warp 0's join and drain run
+    out and the CTA is poisoned (a late helper could still write into its
+    shared memory).  The launch must still end; every cell either succeeds with
+    the one-warp launch's exact results or fails with CV_ERR_FAILURE; cells a
+    poisoned CTA claims afterwards are left as given."""
+    b = _cells(300, seed=9)   # more cells than CTAs (one per SM)
+    ref = _helper_run(b, cta_helpers=0)
+    T, Y, st, nst = _helper_run(b, cta_helpers=1, helper_join_cycles=200, helper_drain_cycles=200,
+                                helper_idle_cycles=500)
+    assert set(np.unique(st)) <= {0, -3}, np.unique(st)
+    assert (st == -3).any()
+    ok = st == 0
+    assert np.array_equal(T[ok], ref[0][ok]) and np.array_equal(Y[:, ok], ref[1][:, ok])
+    assert np.array_equal(nst[ok], ref[3][ok])
+    untouched = (st == -3) & (nst == 0)
+    assert untouched.any()
+    assert np.array_equal(T[untouched], b.T[untouched])
+    assert np.array_equal(Y[:, untouched], b.Y[:, untouched])

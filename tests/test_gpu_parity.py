@@ -111,6 +111,29 @@ def test_integration_matches_oracle(oracle, wl, n, precision):
         assert abs(g - c) <= 0.1 * c + 10, (k, g, c)
 
 
+@pytest.mark.parametrize("wl,n", [("gri_32k", 64), ("h2_1024", 64)])
+def test_refinement_sweep_matches_oracle(oracle, wl, n):
+    """options.refine = 1 (mixed precision): every Newton correction from the
+    FP32 factors gets one refinement sweep, r = b - (I - gamma J) x with the
+    saved Jacobian in FP64 arithmetic, x += M^-1 r.  Same parity gates and
+    counter agreement as the plain mixed form, and the sweep changes the bits of
+    the result (it is not skipped)."""
+    b = W.make(wl, n, seed=31)
+    yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, rtol=W.RTOL, atol=W.ATOL, threads=8)
+    T, Y, st, stats, cnt = run_gpu(b, native.B200ODE_MIXED, counters=True, refine=1)
+    T0, Y0, _, _, cnt0 = run_gpu(b, native.B200ODE_MIXED, counters=True)
+    assert (st == 0).all() and (so["status"] == 0).all()
+    compare(b, T, Y, yo, f"{wl}/refine", oracle)
+    assert np.abs(Y.sum(axis=0) - 1.0).max() < 1e-12
+    for k in ("nst", "nni", "nje", "nsetups"):
+        g, c = cnt[k].sum(), so[k].sum()
+        assert abs(g - c) <= 0.1 * c + 10, (k, g, c)
+    assert not (np.array_equal(T, T0) and np.array_equal(Y, Y0))
+    # deterministic
+    T2, Y2, _, _, _ = run_gpu(b, native.B200ODE_MIXED, refine=1)
+    assert np.array_equal(T, T2) and np.array_equal(Y, Y2)
+
+
 def test_accuracy_vs_fp64_oracle_not_worse_than_cpu(oracle):
     """Error against the FP64 oracle at rtol 1e-10: the GPU (mixed) is as accurate
     as the CPU integrator at the same rtol 1e-6."""
@@ -296,3 +319,77 @@ def test_invalid_arguments_raise():
     with pytest.raises(native.B200Error):
         s.integrate(np.full(2, 1000.0), np.full((53, 2), 1.0 / 53), -1.0, 1e-4)
     s.close()
+
+
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_memory_sized_chunks_equal_one_launch(persistent):
+    """A batch larger than max_cells_per_launch (the memory-sized batching of
+    the reference's calc_gpu_points) runs as consecutive launches over
+    contiguous chunks; cells are independent, so results, statuses, per-cell
+    counters and call totals equal one launch over the whole batch bitwise,
+    through the host-buffer and the device-buffer entry points."""
+    import torch
+    b = W.make("gri_1m", 333, seed=17)
+    out = {}
+    for chunk in (0, 100):
+        s = native.Solver("gri30", precision=native.B200ODE_FP64, persistent=persistent,
+                          max_cells_per_launch=chunk)
+        T, Y = b.T.copy(), np.ascontiguousarray(b.Y.copy())
+        st, stats, cnt = s.integrate(T, Y, b.P, b.dt, counters=True)
+        dT = torch.from_numpy(b.T.copy()).cuda()
+        dY = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
+        dP = torch.from_numpy(np.ascontiguousarray(b.P)).cuda()
+        dst = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
+        dstats = s.integrate_device(b.ncells, dP.data_ptr(), 0.0, dT.data_ptr(), dY.data_ptr(), b.dt,
+                                    dstatus=dst.data_ptr())
+        torch.cuda.synchronize()
+        s.close()
+        out[chunk] = (T, Y, st, cnt, stats, dT.cpu().numpy(), dY.cpu().numpy(), dst.cpu().numpy(), dstats)
+    a, c = out[0], out[100]
+    assert (a[2] == 0).all()
+    for i in (0, 1, 2, 5, 6, 7):
+        assert np.array_equal(a[i], c[i]), i
+    assert np.array_equal(a[0], a[5]) and np.array_equal(a[1], a[6])
+    for k in native.COUNTERS:
+        assert np.array_equal(a[3][k], c[3][k]), k
+    for k in ("total_nst", "total_nfe", "total_nje", "total_nsetups", "total_nni", "n_failed"):
+        assert a[4][k] == c[4][k] == a[8][k] == c[8][k], k
+    assert c[4]["gpu_launches"] > a[4]["gpu_launches"]
+
+
+@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("h2_li_2004", "h2li_grid")])
+@pytest.mark.parametrize("lanes", [16, 8])
+def test_several_cells_per_warp(oracle, mech, wl, lanes):
+    """The H2 mechanisms with 2 or 4 cells per warp (16 or 8 lanes per cell):
+    the right-hand side is bitwise that of one cell per warp (same reaction
+    slots, same gather lists and order, same reduction trees), the integration
+    passes the parity gates against the CPU oracle in both precisions, and the
+    counters track the oracle's."""
+    b = W.make(wl, 333, seed=23)
+    s32 = native.Solver(mech, lanes_per_cell=32)
+    sg = native.Solver(mech, lanes_per_cell=lanes)
+    f32 = s32.eval_rhs(b.T, b.Y, b.P)
+    fg = sg.eval_rhs(b.T, b.Y, b.P)
+    s32.close()
+    sg.close()
+    assert np.array_equal(f32[0], fg[0]) and np.array_equal(f32[1], fg[1])
+    yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, rtol=W.RTOL, atol=W.ATOL, threads=8)
+    for precision in (native.B200ODE_FP64, native.B200ODE_MIXED):
+        T, Y, st, stats, cnt = run_gpu(b, precision, counters=True, lanes_per_cell=lanes)
+        assert (st == 0).all()
+        compare(b, T, Y, yo, f"{mech}/{lanes}/{precision}", oracle)
+        assert np.abs(Y.sum(axis=0) - 1.0).max() < 1e-12
+        for k in ("nst", "nni"):
+            g, c = cnt[k].sum(), so[k].sum()
+            assert abs(g - c) <= 0.1 * c + 10, (k, g, c)
+    # persistent == step form with several cells per warp
+    Tp, Yp, sp, _, _ = run_gpu(b, native.B200ODE_FP64, lanes_per_cell=lanes)
+    Ts, Ys, ss, _, _ = run_gpu(b, native.B200ODE_FP64, persistent=0, lanes_per_cell=lanes)
+    assert np.array_equal(Tp, Ts) and np.array_equal(Yp, Ys) and np.array_equal(sp, ss)
+
+
+def test_lanes_per_cell_is_validated():
+    with pytest.raises(native.B200Error):
+        native.Solver("gri30", lanes_per_cell=16)
+    with pytest.raises(native.B200Error):
+        native.Solver("h2o2", lanes_per_cell=12)

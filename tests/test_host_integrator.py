@@ -101,3 +101,30 @@ def test_reacting_cells_match_c_abi(driver, wl, mech, opts, precision):
     s.close()
     assert np.array_equal(st, st2)
     assert np.array_equal(To, T) and np.array_equal(Yo, Y.T)
+
+
+def test_integrator_compiles_against_the_reference_headers(tmp_path):
+    """B200BDFIntegrator built with -DB200ODE_WITH_REFERENCE_HEADERS includes the
+    reference's own include/ODEIntegrator/Integrators/Integrator.hpp (and through
+    it Mesh, Logger and Context) instead of the restated interface; its
+    `override`s must bind to the reference's virtuals init / integrate / clean
+    (Integrator.hpp:22-40).  yaml-cpp is not installed, so a stand-in declaring
+    the YAML::Node surface the integrator touches (tests/cpp/stub_include) takes
+    its place.  Compiled to an object file; skipped without the reference."""
+    import os
+    import subprocess
+    from oracle.refpath import reference_subdir
+    inc = reference_subdir("include")
+    if inc is None or not os.path.exists(os.path.join(inc, "ODEIntegrator", "Integrators", "Integrator.hpp")):
+        pytest.skip("reference headers not present")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "hpc_ode_b200", "csrc", "host", "b200_bdf_integrator.cpp")
+    out = subprocess.run(["g++", "-std=c++17", "-c", "-DB200ODE_WITH_REFERENCE_HEADERS",
+                          "-I", os.path.join(root, "include"), "-I", os.path.join(root, "tests", "cpp", "stub_include"),
+                          "-I", inc, src, "-o", str(tmp_path / "integrator_ref.o")],
+                         capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr[-3000:]
+    syms = subprocess.run(["nm", "-C", str(tmp_path / "integrator_ref.o")], capture_output=True, text=True).stdout
+    for fn in ("B200BDFIntegrator::init(std::shared_ptr<Context>, IntegratorConfig)",
+               "B200BDFIntegrator::integrate(double, double)", "B200BDFIntegrator::clean()"):
+        assert fn in syms, fn

@@ -72,3 +72,40 @@ def test_gloo_world2_equals_single_process(tmp_path):
     T, Y = b.T.copy(), b.Y.copy()
     st = _fake_integrate(T, Y, b.P, b.dt)
     assert np.array_equal(r["T"], T) and np.array_equal(r["Y"], Y) and np.array_equal(r["st"], st)
+
+
+def _strong_worker(rank, world, port, out):
+    """bench.py --scaling strong's split, on gloo ranks: every rank builds the
+    same seeded workload, takes its cost-balanced range (shard.rank_range) as a
+    subset batch, integrates it (fake per-cell map) and the parts are gathered."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    full = W.make("gri_1m", 4096, seed=5)
+    a, b = shard.rank_range(full.T, world, rank)
+    part = full.subset(np.arange(a, b))
+    T, Y = part.T.copy(), np.ascontiguousarray(part.Y.copy())
+    st = _fake_integrate(T, Y, part.P, part.dt)
+    res = shard.gather_to(0, slice(a, b), T, Y, st, full.ncells)
+    ranges = [None] * world if rank == 0 else None
+    dist.gather_object((a, b), ranges, dst=0)
+    if rank == 0:
+        np.savez(out, T=res[0], Y=res[1], st=res[2], ranges=np.array(ranges))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_strong_scaling_split_gloo_world2(tmp_path):
+    out = str(tmp_path / "strong.npz")
+    mp.start_processes(_strong_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    r = np.load(out)
+    full = W.make("gri_1m", 4096, seed=5)
+    want = shard.balanced_ranges(shard.temperature_cost(full.T), 2)
+    assert [tuple(x) for x in r["ranges"]] == want
+    assert want[0][1] == want[1][0] and 0 < want[0][1] < full.ncells
+    cost = shard.temperature_cost(full.T)
+    s0, s1 = cost[:want[0][1]].sum(), cost[want[0][1]:].sum()
+    assert abs(s0 - s1) <= 2 * cost.max()
+    T, Y = full.T.copy(), full.Y.copy()
+    st = _fake_integrate(T, Y, full.P, full.dt)
+    assert np.array_equal(r["T"], T) and np.array_equal(r["Y"], Y) and np.array_equal(r["st"], st)
