@@ -687,6 +687,7 @@ template <class MT, class LinT>
 __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A_off, unsigned chem_off,
                                       JacScratch<MT>* js, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
+    static_assert(3 * N <= MT::NSLOT, "the per-species work [3][N] reuses the rate buffer q[NSLOT]");
     const unsigned gm = gmask<G>();
     const DevMech& M = mech<MT>();
     LinT* A = smem_at<LinT>(A_off);

@@ -103,8 +103,59 @@ static int check(const GenTables& g, int nunits_generated, int nplog_generated) 
         if (inert[k] != (reacts ? 0 : 1)) { std::printf("FAIL %s: inert flag of species %d\n", g.name, k); return 1; }
         ninert += inert[k];
     }
-    std::printf("ok %s nslot %d nunit %d gmax %d plog %d inert %d nu_den %d\n", g.name, ns, h.nunit, h.gmax, nplog,
-                ninert, g.nu_den);
+    // every table-derived index the kernels use, against the array it indexes
+    // (the device code does not check them): reaction factor species index the
+    // concentrations / Gibbs terms C[0..N] (N = the padding factor 1 / 0),
+    // Jacobian scatter rows and third-body species index rows/columns 0..N-1,
+    // third-body lists stay inside tb_sp, catalysts are species, gather words
+    // address slots 0..nslot-1 and units 0..NUNITS-1, each species' units are a
+    // contiguous in-range run, PLOG slots' levels and terms stay in their tables;
+    // and the Jacobian's per-species work ([3][N] doubles) fits the rate buffer
+    // (nslot doubles) it reuses.
+    auto bad = [&](const char* what, int s, int v) {
+        std::printf("FAIL %s: %s (slot %d, value %d)\n", g.name, what, s, v);
+        return 1;
+    };
+    const int* rf = at<int>(h, h.o_rf);
+    const int* pf = at<int>(h, h.o_pf);
+    const int* tb_off = at<int>(h, h.o_tb_off);
+    const int* tb_len = at<int>(h, h.o_tb_len);
+    const int* tb_sp = at<int>(h, h.o_tb_sp);
+    const int* cat_sp = at<int>(h, h.o_cat_sp);
+    const int* jrow = at<int>(h, h.o_jrow);
+    const int* plev0 = at<int>(h, h.o_plog_lev0);
+    const int* pnlev = at<int>(h, h.o_plog_nlev);
+    const int* ptoff = at<int>(h, h.o_plog_toff);
+    for (int s = 0; s < ns; ++s) {
+        for (int a = 0; a < 3; ++a) {
+            if (rf[a * ns + s] < 0 || rf[a * ns + s] > n) return bad("reactant factor species", s, rf[a * ns + s]);
+            if (pf[a * ns + s] < 0 || pf[a * ns + s] > n) return bad("product factor species", s, pf[a * ns + s]);
+        }
+        if (tb_off[s] < 0 || tb_len[s] < 0 || tb_off[s] + tb_len[s] > h.ntb) return bad("third-body list", s, tb_off[s]);
+        for (int t = 0; t < tb_len[s]; ++t)
+            if (tb_sp[tb_off[s] + t] < 0 || tb_sp[tb_off[s] + t] >= n) return bad("third-body species", s, tb_sp[tb_off[s] + t]);
+        if ((flags[s] & b200::kFlagCatalyst) && (cat_sp[s] < 0 || cat_sp[s] >= n)) return bad("catalyst", s, cat_sp[s]);
+        for (int e = 0; e < b200::kJRow; ++e) {
+            const int k = jrow[e * ns + s];
+            if (k < -1 || k >= n) return bad("Jacobian row", s, k);
+        }
+        if (flags[s] & b200::kFlagPlog) {
+            if (plev0[s] < 0 || pnlev[s] < 1 || plev0[s] + pnlev[s] > g.nplog_lev) return bad("PLOG levels", s, plev0[s]);
+            for (int l = plev0[s]; l < plev0[s] + pnlev[s]; ++l)
+                if (ptoff[l] < 0 || ptoff[l + 1] < ptoff[l] || ptoff[l + 1] > g.nplog_term) return bad("PLOG terms", s, l);
+        }
+    }
+    for (int e = 0; e < h.gmax; ++e)
+        for (int l = 0; l < 32; ++l) {
+            const int w = gword[e * 32 + l];
+            if ((w & 2047) >= ns) return bad("gather slot", e, w & 2047);
+            if ((w >> 17) >= nunits_generated) return bad("gather unit", e, w >> 17);
+        }
+    for (int k = 0; k < n; ++k)
+        if (unit_off[k] < 0 || unit_off[k + 1] < unit_off[k] || unit_off[k + 1] > h.nunit) return bad("species units", k, unit_off[k]);
+    if (3 * n > ns) return bad("Jacobian per-species work [3][N] exceeds the rate buffer", ns, 3 * n);
+    std::printf("ok %s nslot %d nunit %d gmax %d plog %d inert %d nu_den %d (indices in range)\n", g.name, ns, h.nunit,
+                h.gmax, nplog, ninert, g.nu_den);
     return 0;
 }
 

@@ -110,7 +110,10 @@ def test_device_table_packing(tmp_path):
     every compiled mechanism; its gather-unit count equals the generated
     NUNITS the kernels size their shared scratch by, its gather words
     reproduce each net stoichiometric coefficient (fractional ones included),
-    and PLOG slots and inert species agree with the tables."""
+    PLOG slots and inert species agree with the tables, and every index the
+    kernels read from the tables (factor species, third-body lists, catalysts,
+    Jacobian rows, gather slots and units, PLOG levels and terms) lies inside
+    the array it indexes."""
     import subprocess
     here = os.path.dirname(os.path.abspath(__file__))
     exe = tmp_path / "pack_check"
@@ -119,6 +122,6 @@ def test_device_table_packing(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0, out.stdout
     lines = out.stdout.strip().splitlines()
-    assert len(lines) == 5 and all(l.startswith("ok ") for l in lines)
+    assert len(lines) == 5 and all(l.startswith("ok ") and "indices in range" in l for l in lines)
     est = [l for l in lines if "estimate" in l][0]
     assert "plog 22" in est and "nu_den 2" in est
