@@ -355,7 +355,6 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2, help="timed end-to-end calls (after one warm-up call)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (launch shape, threads per cell, queue chunk) before warm-up")
-    ap.add_argument("--lanes-per-cell", type=int, default=0, help="threads per cell (0 = mechanism default)")
     ap.add_argument("--accuracy-cells", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -401,7 +400,7 @@ def main():
     prec = native.B200ODE_MIXED if args.precision == "mixed" else native.B200ODE_FP64
     form = native.B200ODE_CONV if args.formulation == "conv" else native.B200ODE_CONP
     solver = native.Solver(batch.mech, precision=prec, persistent=int(args.form == "persistent"),
-                           device=dev.index, formulation=form, lanes_per_cell=args.lanes_per_cell)
+                           device=dev.index, formulation=form)
     nsp = solver.nsp
     T0 = torch.from_numpy(batch.T).to(dev)
     Y0 = torch.from_numpy(np.ascontiguousarray(batch.Y)).to(dev)
@@ -419,7 +418,7 @@ def main():
         t_at = time.perf_counter()
         solver.autotune(n, P.data_ptr(), 0.0, T0.data_ptr(), Y0.data_ptr(), batch.dt)
         o = solver.options()
-        tuned = {"lanes_per_cell": o.lanes_per_cell, "warps_per_block": o.warps_per_block,
+        tuned = {"warps_per_block": o.warps_per_block,
                  "blocks_per_sm": o.blocks_per_sm, "queue_chunk": o.queue_chunk, "cta_helpers": o.cta_helpers,
                  "seconds": time.perf_counter() - t_at}
     opts_used = solver.options()
@@ -600,8 +599,7 @@ def main():
                    "precision": args.precision, "form": args.form, "formulation": args.formulation,
                    "l2": "256 MiB memset between timed steps",
                    "parallelism": f"cell shards x{ws} ({args.scaling}), no collective",
-                   "launch": {"lanes_per_cell": opts_used.lanes_per_cell,
-                              "warps_per_block": opts_used.warps_per_block,
+                   "launch": {"warps_per_block": opts_used.warps_per_block,
                               "blocks_per_sm": opts_used.blocks_per_sm, "queue_chunk": opts_used.queue_chunk,
                               "autotuned": tuned}},
         "kernel_ms_per_step": kernel_ms,

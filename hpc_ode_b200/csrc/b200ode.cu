@@ -69,14 +69,12 @@ b200ode_status fail(b200ode_status st, const std::string& msg) {
 
 enum MechId { MECH_GRI30 = 0, MECH_H2O2 = 1, MECH_NDODECANE = 2, MECH_H2LI = 3, MECH_ESTIMATE = 4 };
 
-// Traits of each compiled mechanism, per formulation (CV = 1: constant
-// volume) and, for the two H2 mechanisms (9-10 unknowns), lanes per cell.
+// Traits of each compiled mechanism, per formulation (CV = 1: constant volume).
 #define MECH_TRAITS(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG, CV>
-#define MECH_TRAITS_G(PFX, ID) MechT<PFX##_NSP, PFX##_NRXN, ID, PFX##_NU_DEN, PFX##_NUNITS, PFX##_NPLOG, CV, G>
 template <int CV> using GriF = MECH_TRAITS(MECH_GRI30, MECH_GRI30);
-template <int CV, int G = 32> using H2F = MECH_TRAITS_G(MECH_H2O2, MECH_H2O2);
+template <int CV> using H2F = MECH_TRAITS(MECH_H2O2, MECH_H2O2);
 template <int CV> using NdF = MECH_TRAITS(MECH_NDODECANE_REITZ, MECH_NDODECANE);
-template <int CV, int G = 32> using H2LiF = MECH_TRAITS_G(MECH_H2_LI_2004, MECH_H2LI);
+template <int CV> using H2LiF = MECH_TRAITS(MECH_H2_LI_2004, MECH_H2LI);
 // kerosene (214 species): mixed precision only -- one warp's FP32 Newton
 // matrix (214 x 215 x 4 B = 184 KB) fills an SM's shared memory; the FP64
 // matrix would not fit
@@ -87,9 +85,6 @@ using NdT = NdF<0>;
 using H2LiT = H2LiF<0>;
 using EstT = EstF<0>;
 static_assert(MECH_ESTIMATE + 1 == kNumMech, "one descriptor per mechanism");
-
-// Lanes per cell the H2 mechanisms use unless the options say otherwise.
-constexpr int kSmallMechLanes = 16;
 
 int mech_from_name(const char* name) {
     if (!name) return -1;
@@ -643,14 +638,7 @@ b200ode_status dispatch_form(const b200ode_handle* h, F&& f) {
     if (h->mech == MECH_GRI30) return fp64 ? f(GriF<CV>{}, double{}) : f(GriF<CV>{}, float{});
     if (h->mech == MECH_NDODECANE) return fp64 ? f(NdF<CV>{}, double{}) : f(NdF<CV>{}, float{});
     if (h->mech == MECH_ESTIMATE) return f(EstF<CV>{}, float{});   // FP64 refused at creation
-    const int g = h->opt.lanes_per_cell;   // resolved at creation: 32, 16 or 8 for the H2 mechanisms
-    if (h->mech == MECH_H2LI) {
-        if (g == 8) return fp64 ? f(H2LiF<CV, 8>{}, double{}) : f(H2LiF<CV, 8>{}, float{});
-        if (g == 16) return fp64 ? f(H2LiF<CV, 16>{}, double{}) : f(H2LiF<CV, 16>{}, float{});
-        return fp64 ? f(H2LiF<CV>{}, double{}) : f(H2LiF<CV>{}, float{});
-    }
-    if (g == 8) return fp64 ? f(H2F<CV, 8>{}, double{}) : f(H2F<CV, 8>{}, float{});
-    if (g == 16) return fp64 ? f(H2F<CV, 16>{}, double{}) : f(H2F<CV, 16>{}, float{});
+    if (h->mech == MECH_H2LI) return fp64 ? f(H2LiF<CV>{}, double{}) : f(H2LiF<CV>{}, float{});
     return fp64 ? f(H2F<CV>{}, double{}) : f(H2F<CV>{}, float{});
 }
 
@@ -904,7 +892,6 @@ void b200ode_default_options(b200ode_options* o) {
     o->helper_drain_cycles = 0;
     o->helper_idle_cycles = 0;
     o->max_cells_per_launch = 0;
-    o->lanes_per_cell = 0;
 }
 
 const char* b200ode_last_error(void) { return g_last_error.c_str(); }
@@ -944,12 +931,6 @@ b200ode_status b200ode_create(const char* mech_name, const b200ode_options* opts
         return fail(B200ODE_ERR_INVALID, "precision must be B200ODE_FP64 or B200ODE_MIXED");
     if (o.formulation != B200ODE_CONP && o.formulation != B200ODE_CONV)
         return fail(B200ODE_ERR_INVALID, "formulation must be B200ODE_CONP or B200ODE_CONV");
-    // lanes per cell: 32 (a warp per cell) for every mechanism; the two H2
-    // mechanisms (9-10 unknowns) also run 2 or 4 cells per warp
-    const bool small_mech = (mech == MECH_H2O2 || mech == MECH_H2LI);
-    if (o.lanes_per_cell == 0) o.lanes_per_cell = small_mech ? kSmallMechLanes : 32;
-    if (o.lanes_per_cell != 32 && !(small_mech && (o.lanes_per_cell == 16 || o.lanes_per_cell == 8)))
-        return fail(B200ODE_ERR_INVALID, "lanes_per_cell must be 0 or 32 (or 16 / 8 for h2o2 and h2_li_2004)");
     if (mech == MECH_ESTIMATE && o.precision == B200ODE_FP64)
         return fail(B200ODE_ERR_INVALID,
                     "ESTiMatE-Mech_04042022 (214 unknowns) runs in B200ODE_MIXED only: its FP64 Newton "
@@ -1251,7 +1232,6 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     if (rc != B200ODE_OK) return rc;
     if (n <= 0 || !dT || !dY) return fail(B200ODE_ERR_INVALID, "autotune needs cells (device T and Y)");
     if (!dP && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
-    const bool small_mech = (h->mech == MECH_H2O2 || h->mech == MECH_H2LI);
     const bool wide_mech = (h->mech == MECH_ESTIMATE);   // one cell per SM: helper warps on or off
     // the sample: the first m cells (a few per SM for the widest mechanism, whose
     // cells take seconds), copied so the caller's buffers stay untouched
@@ -1293,28 +1273,24 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
         *out_ms = ms_c;
         return B200ODE_OK;
     };
-    // stage 1, the launch shape: lanes per cell (32, or 16 / 8 for the H2
-    // mechanisms) x warps per CTA (4, 2, 1) x register variant (blocks_per_sm >=
-    // 3 * 4 / wpb selects the 168-register variant, which trades spills for
-    // resident warps) x helper warps (widest mechanism); shapes whose shared
-    // memory exceeds a CTA's are skipped
-    struct Cand { int lanes, wpb, bps, helpers, chunk; };
+    // stage 1, the launch shape: warps per CTA (4, 2, 1) x register variant
+    // (blocks_per_sm >= 3 * 4 / wpb selects the 168-register variant, which
+    // trades spills for resident warps) x threads per cell for the widest
+    // mechanism (a 4-warp CTA per cell with helper warps, or one warp); shapes
+    // whose shared memory exceeds a CTA's are skipped
+    struct Cand { int wpb, bps, helpers, chunk; };
     std::vector<Cand> shapes;
-    for (int lanes : {32, 16, 8}) {
-        if (lanes != 32 && !small_mech) continue;
-        for (int wpb : {4, 2, 1})
-            for (int v = 0; v < 2; ++v)
-                for (int helpers : {1, 0}) {
-                    if (helpers == 0 && !(wide_mech && wpb == 1)) continue;
-                    shapes.push_back({lanes, wpb, v ? 3 * (4 / wpb) : 0, helpers, 1});
-                }
-    }
+    for (int wpb : {4, 2, 1})
+        for (int v = 0; v < 2; ++v)
+            for (int helpers : {1, 0}) {
+                if (helpers == 0 && !(wide_mech && wpb == 1)) continue;
+                shapes.push_back({wpb, v ? 3 * (4 / wpb) : 0, helpers, 1});
+            }
     float best_ms = 0.f;
-    Cand best{0, 0, 0, 0, 0};
+    Cand best{0, 0, 0, 0};
     bool have = false;
     for (const Cand& c : shapes) {
         if (rc != B200ODE_OK) break;
-        h->opt.lanes_per_cell = c.lanes;
         h->opt.warps_per_block = c.wpb;
         h->opt.blocks_per_sm = c.bps;
         h->opt.cta_helpers = c.helpers;
@@ -1336,7 +1312,6 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     // stage 2, the work-queue chunk (cells a warp claims per queue access) on
     // the chosen shape
     if (rc == B200ODE_OK && have) {
-        h->opt.lanes_per_cell = best.lanes;
         h->opt.warps_per_block = best.wpb;
         h->opt.blocks_per_sm = best.bps;
         h->opt.cta_helpers = best.helpers;
@@ -1357,7 +1332,6 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     h->opt = saved;
     if (rc != B200ODE_OK) return rc;
     if (!have) return fail(B200ODE_ERR_CUDA, "autotune: no launch shape fits this device");
-    h->opt.lanes_per_cell = best.lanes;
     h->opt.warps_per_block = best.wpb;
     h->opt.blocks_per_sm = best.bps;
     h->opt.cta_helpers = best.helpers;

@@ -299,12 +299,16 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
                       ((cf == cv::FAIL_BAD_J) && (dgamma < cv::DGMAX_JBAD)) || (cf == cv::FAIL_OTHER);
     LinT* A = w->A;
     LinT* J = wg->savedJ;
-    if (!jbad) {
+    // M = I - gamma J, fused with the copy from (or to) the saved Jacobian in
+    // global memory (mostly L2 resident): rows go in batches whose loads are all
+    // issued before any store, so their latencies overlap instead of adding up
+    // element by element.  Lane j owns columns j, j + G, ...: every element is
+    // read and written by the same lane.
+    constexpr int kB = (MT::NS <= 2) ? 8 : ((16 / MT::NS) > 1 ? 16 / MT::NS : 1);
+    const LinT mg = (LinT)(-S.gamma);
+    const bool from_saved = !jbad;
+    if (from_saved) {
         S.jcur = 0;
-#pragma unroll 1
-        for (int i = 0; i < N; ++i)
-            #pragma unroll 1
-            for (int j = lane; j < N; j += MT::G) A[i * LDA + j] = J[i * N + j];
     } else {
         S.cnt[C_NJE]++;
         S.nstlj = S.nst;
@@ -312,21 +316,30 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
         const long long tj = ph_tick(S);
         warp_jac<MT, LinT>(S.P, yv, smem_off(A), smem_off(&w->chem), &wg->js, lane);
         ph_tock(S, PH_JAC, tj, lane);
-#pragma unroll 1
-        for (int i = 0; i < N; ++i)
-            #pragma unroll 1
-            for (int j = lane; j < N; j += MT::G) J[i * N + j] = A[i * LDA + j];
     }
-    __syncwarp(gmask<MT::G>());
-    const LinT mg = (LinT)(-S.gamma);
 #pragma unroll 1
-    for (int i = 0; i < N; ++i)
-        #pragma unroll 1
-        for (int j = lane; j < N; j += MT::G) {
-            LinT v = mg * A[i * LDA + j];
-            if (i == j) v += LinT(1);
-            A[i * LDA + j] = v;
-        }
+    for (int i0 = 0; i0 < N; i0 += kB) {
+        LinT v[kB][MT::NS];
+#pragma unroll
+        for (int r = 0; r < kB; ++r)
+#pragma unroll
+            for (int s = 0; s < MT::NS; ++s) {
+                const int i = i0 + r, j = lane + MT::G * s;
+                v[r][s] = (i < N && j < N) ? (from_saved ? J[i * N + j] : A[i * LDA + j]) : LinT(0);
+            }
+#pragma unroll
+        for (int r = 0; r < kB; ++r)
+#pragma unroll
+            for (int s = 0; s < MT::NS; ++s) {
+                const int i = i0 + r, j = lane + MT::G * s;
+                if (i < N && j < N) {
+                    if (!from_saved) J[i * N + j] = v[r][s];
+                    LinT x = mg * v[r][s];
+                    if (i == j) x += LinT(1);
+                    A[i * LDA + j] = x;
+                }
+            }
+    }
     __syncwarp(gmask<MT::G>());
     S.lu_dirty = 1;
     const long long tl = ph_tick(S);

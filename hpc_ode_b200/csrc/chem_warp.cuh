@@ -41,11 +41,11 @@ constexpr double kRU = 8314.4621;
 // formulation: constant pressure, or constant volume (CONV_ = 1; the kernels'
 // pressure slot then carries the cell's fixed density).  Both are compile-time
 // so a kernel holds no code of the other case.  G_ is the number of lanes that
-// integrate one cell: 32 (a warp per cell), or 16 / 8 for the smallest
-// mechanisms, whose 9-10 species leave most of a warp idle in every vector
-// phase; then 2 or 4 cells share a warp, each on its aligned group of G lanes
-// (shuffles, votes and syncs take the group's mask), and the scalar step logic
-// every lane of a group repeats is issued once for all cells of the warp.
+// integrate one cell; the device code takes every shuffle, vote and sync over
+// the cell's aligned group of G lanes.  All compiled kernels use G = 32 (a warp
+// per cell): 2 or 4 cells per warp for the 9-10-species H2 mechanisms ran
+// slower than one (the cells' step logic diverges, and the extra registers
+// cost resident warps), so those instances are not built.
 template <int N_, int NR_, int ID_, int NU_DEN_, int NUNITS_, int NPLOG_, int CONV_ = 0, int G_ = 32>
 struct MechT {
     static_assert(G_ == 32 || G_ == 16 || G_ == 8, "lanes per cell: 32, 16 or 8");
@@ -846,14 +846,15 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
         trow[s] = 0.0;
         if (j < N - 1) {
             double S1 = 0.0;
-#pragma unroll 1
+#pragma unroll 4
             for (int k = 0; k < N; ++k) S1 += spw[k] * (double)A[k * LDA + j];
             const double iWj = __ldg(M.inv_mw + j);
             trow[s] = -(S1 * iWj - S2 * iWN + (iWj - iWN) * S3 + fT * (spw[N + j] - spw[N + N - 1])) * inv_cp;
         }
     }
     __syncwarp(gm);
-    // species rows k < N-1 (lane owns rows), then the T column
+    // species rows k < N-1 (lane owns rows), then the T column; each row goes
+    // in batches of 8 columns whose loads are issued before their stores
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
         const int k = lane + G * s;
@@ -862,10 +863,20 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
             const double Wk = __ldg(M.mw + k);
             const double cN = (double)row[N - 1] * iWN;
             const double X = spw[2 * N + k];
+            constexpr int kB = 8;
 #pragma unroll 1
-            for (int j = 0; j < N - 1; ++j) {
-                const double iWj = __ldg(M.inv_mw + j);
-                row[j] = (LinT)(Wk * ((double)row[j] * iWj - cN + X * (iWj - iWN)));
+            for (int j0 = 0; j0 < N - 1; j0 += kB) {
+                LinT a[kB];
+                double iw[kB];
+#pragma unroll
+                for (int r = 0; r < kB; ++r) {
+                    const int j = j0 + r < N - 1 ? j0 + r : N - 2;
+                    a[r] = row[j];
+                    iw[r] = __ldg(M.inv_mw + j);
+                }
+#pragma unroll
+                for (int r = 0; r < kB; ++r)
+                    if (j0 + r < N - 1) row[j0 + r] = (LinT)(Wk * ((double)a[r] * iw[r] - cN + X * (iw[r] - iWN)));
             }
             row[N - 1] = (LinT)dfdT[s];
         }

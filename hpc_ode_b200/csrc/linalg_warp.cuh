@@ -293,42 +293,15 @@ __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off
         if (lane == 0) dinv[k] = inv;
         for (int i = k + 1 + lane; i < N; i += G) A[i * LDA + k] *= inv;
         __syncwarp(gm);
-        // rank-1 update of the trailing block; lane owns columns j = lane + G s > k.
-        // Rows go in batches of kRows whose multipliers and entries are all
-        // loaded before any store (a load may not pass a store to the same
-        // array, so element-by-element updates would each wait out the full
-        // shared-memory latency); every element gets the same single fused
-        // multiply-add as in the element-by-element form.
-        constexpr int kRows = 8;
-        LinT u[NS];
-        bool on[NS];
-        bool any = false;
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int j = lane + G * s;
-            u[s] = (j > k && j < N) ? A[k * LDA + j] : LinT(0);
-            on[s] = u[s] != LinT(0);
-            any = any || on[s];
-        }
-        if (__any_sync(gm, any)) {
-#pragma unroll 1
-            for (int i0 = k + 1; i0 < N; i0 += kRows) {
-                LinT l[kRows];
-#pragma unroll
-                for (int r = 0; r < kRows; ++r) l[r] = (i0 + r < N) ? A[(i0 + r) * LDA + k] : LinT(0);
-#pragma unroll
-                for (int s = 0; s < NS; ++s) {
-                    if (on[s]) {
-                        const int j = lane + G * s;
-                        LinT a[kRows];
-#pragma unroll
-                        for (int r = 0; r < kRows; ++r)
-                            if (i0 + r < N) a[r] = A[(i0 + r) * LDA + j];
-#pragma unroll
-                        for (int r = 0; r < kRows; ++r)
-                            if (i0 + r < N) A[(i0 + r) * LDA + j] = a[r] - l[r] * u[s];
-                    }
-                }
+        // rank-1 update of the trailing block; lane owns columns j.  (Batching
+        // each column's loads ahead of its stores measured neutral for GRI-Mech
+        // 3.0 and cost the 10-species mechanisms a third of their resident warps
+        // through the registers it takes, so the element-wise form stays.)
+        for (int j = k + 1 + lane; j < N; j += G) {
+            const LinT ukj = A[k * LDA + j];
+            if (ukj != LinT(0)) {
+#pragma unroll 4
+                for (int i = k + 1; i < N; ++i) A[i * LDA + j] -= A[i * LDA + k] * ukj;
             }
         }
         __syncwarp(gm);

@@ -54,8 +54,7 @@ class Options(C.Structure):
                 ("use_graph", C.c_int32), ("device", C.c_int32), ("profile_phases", C.c_int32),
                 ("formulation", C.c_int32), ("cta_helpers", C.c_int32),
                 ("helper_join_cycles", C.c_int64), ("helper_drain_cycles", C.c_int64),
-                ("helper_idle_cycles", C.c_int64), ("max_cells_per_launch", C.c_int64),
-                ("lanes_per_cell", C.c_int32)]
+                ("helper_idle_cycles", C.c_int64), ("max_cells_per_launch", C.c_int64)]
 
 
 _i32p = C.POINTER(C.c_int32)

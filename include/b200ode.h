@@ -102,12 +102,6 @@ typedef struct {
        sizes its batches).  A larger call runs as consecutive launches over contiguous
        chunks of cells; results do not depend on the chunking. */
     int64_t max_cells_per_launch;
-    /* Lanes of a warp that integrate one cell (0 = the mechanism's default): 32 (one cell per
-       warp) for every mechanism; the H2 mechanisms (h2o2, h2_li_2004: 9-10 unknowns) also
-       take 16 or 8 (2 or 4 cells per warp), which the autotuner may pick.  The right-hand
-       side is bitwise the same for every choice; the Jacobian's shared-memory accumulation
-       order is not, so results agree to within the integration tolerances, not bitwise. */
-    int32_t lanes_per_cell;
 } b200ode_options;
 
 /* Optional per-cell counters (CVodeGetNum* equivalents) and call totals.  Any
@@ -248,16 +242,16 @@ b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n_cells, 
  * 8192), or two per SM for the 214-species mechanism; device buffers as
  * b200ode_integrate_device, left unmodified) with the persistent kernel and
  * keeps the fastest choice in the handle's options, which later calls on this
- * handle use.  Stage 1 times every launch shape: threads per cell (a warp, or
- * for the H2 mechanisms 16 or 8 lanes -- 2 or 4 cells per warp; for the
- * 214-species mechanism one 4-warp CTA per cell or one warp) x 4, 2 or 1 warps
- * per CTA x the full-register or the 168-register kernel variant, skipping
- * shapes whose shared memory exceeds a CTA's; stage 2 times the work-queue
- * chunk (1, 2 or 8 cells per claim) on the chosen shape.  The chosen
+ * handle use.  Stage 1 times every launch shape: 4, 2 or 1 warps (cells) per
+ * CTA x the full-register or the 168-register kernel variant, and for the
+ * 214-species mechanism also the threads per cell (one 4-warp CTA per cell
+ * with helper warps, or one warp), skipping shapes whose shared memory exceeds
+ * a CTA's; stage 2 times the work-queue chunk (1, 2 or 8 cells per claim) on
+ * the chosen shape.  Results do not depend on any of these choices.  The chosen
  * warps_per_block and blocks_per_sm are also returned (either pointer may be
- * NULL); b200ode_get_options returns all of them (lanes_per_cell, cta_helpers,
- * queue_chunk).  No reference counterpart: MAGMA's batched LU picks its kernel
- * by a fixed size crossover (ext/magma-2.6.2/control/get_batched_crossover.cpp). */
+ * NULL); b200ode_get_options returns all of them (cta_helpers, queue_chunk
+ * included).  No reference counterpart: MAGMA's batched LU picks its kernel by
+ * a fixed size crossover (ext/magma-2.6.2/control/get_batched_crossover.cpp). */
 b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n_cells, const double* d_P, double P_scalar,
                                 const double* d_T, const double* d_Y, double t0, double t1,
                                 int32_t* warps_per_block, int32_t* blocks_per_sm);

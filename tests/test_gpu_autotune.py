@@ -1,9 +1,7 @@
 """The autotuner (b200ode_autotune): it leaves the sample cells untouched,
-picks one of its candidates (threads per cell, warps per CTA, register variant,
-helper warps, work-queue chunk), and integration results do not depend on the
-launch shape (bitwise for one warp per cell; within the parity gates when the
-H2 mechanisms put several cells in a warp, whose Jacobian accumulates in another
-order)."""
+picks one of its candidates (warps per CTA, register variant, threads per cell
+for the widest mechanism, work-queue chunk), and integration results do not
+depend on the launch shape (bitwise)."""
 import numpy as np
 import pytest
 
@@ -25,7 +23,7 @@ def test_autotune_picks_a_shape_and_results_do_not_change(precision):
     torch.cuda.synchronize()
     assert (wpb, bps) in {(4, 0), (2, 0), (1, 0), (4, 3), (2, 6), (1, 12)}
     o = s.options()
-    assert o.lanes_per_cell == 32 and o.queue_chunk in (1, 2, 8)
+    assert o.queue_chunk in (1, 2, 8)
     assert (o.warps_per_block, o.blocks_per_sm) == (wpb, bps)
     assert torch.equal(T, T0) and torch.equal(Y, Y0)          # sample left untouched
     st = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
@@ -66,29 +64,25 @@ def test_autotune_skips_shapes_that_do_not_fit():
     assert torch.equal(T, T2) and torch.equal(Y, Y2)
 
 
-def test_autotune_h2_tries_several_cells_per_warp(oracle):
-    """The 10-species H2 mechanism: threads per cell 32, 16 or 8 (1, 2 or 4 cells
-    per warp) are candidates; whichever is kept, the integration passes the
-    parity gates against the CPU oracle."""
+def test_autotune_h2_keeps_results_bitwise():
+    """The 10-species H2 mechanism: whichever shape and queue chunk the
+    autotuner keeps, the integration equals the default launch bitwise."""
     import torch
     b = W.make("h2_1024", 4096, seed=19)
     T = torch.from_numpy(b.T.copy()).cuda()
     Y = torch.from_numpy(np.ascontiguousarray(b.Y)).cuda()
     P = torch.from_numpy(b.P.copy()).cuda()
+    T0, Y0 = T.clone(), Y.clone()
     s = native.Solver(b.mech)
     s.autotune(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt)
-    o = s.options()
-    assert o.lanes_per_cell in (32, 16, 8) and o.queue_chunk in (1, 2, 8)
+    assert s.options().queue_chunk in (1, 2, 8)
     st = torch.zeros(b.ncells, dtype=torch.int32, device="cuda")
     s.integrate_device(b.ncells, P.data_ptr(), 0.0, T.data_ptr(), Y.data_ptr(), b.dt, dstatus=st.data_ptr())
     s.close()
+    ref = native.Solver(b.mech)
+    T2, Y2 = T0.clone(), Y0.clone()
+    ref.integrate_device(b.ncells, P.data_ptr(), 0.0, T2.data_ptr(), Y2.data_ptr(), b.dt)
+    ref.close()
     torch.cuda.synchronize()
     assert (st == 0).all()
-    idx = np.arange(0, b.ncells, 16)
-    sub = b.subset(idx)
-    yo, so = oracle.bdf(sub.mech, sub.state_rows(), sub.P, sub.dt, threads=8)
-    Tg = T.cpu().numpy()[idx]
-    Yg = Y.cpu().numpy()[:-1, idx].T
-    assert (np.abs(Tg - yo[:, 0]) / yo[:, 0]).max() <= 1e-5
-    ok = np.abs(Yg - yo[:, 1:]) <= np.maximum(1e-4 * np.abs(yo[:, 1:]), 1e-10)
-    assert ok.mean() >= 0.99
+    assert torch.equal(T, T2) and torch.equal(Y, Y2)

@@ -355,41 +355,3 @@ def test_memory_sized_chunks_equal_one_launch(persistent):
     for k in ("total_nst", "total_nfe", "total_nje", "total_nsetups", "total_nni", "n_failed"):
         assert a[4][k] == c[4][k] == a[8][k] == c[8][k], k
     assert c[4]["gpu_launches"] > a[4]["gpu_launches"]
-
-
-@pytest.mark.parametrize("mech,wl", [("h2o2", "h2_1024"), ("h2_li_2004", "h2li_grid")])
-@pytest.mark.parametrize("lanes", [16, 8])
-def test_several_cells_per_warp(oracle, mech, wl, lanes):
-    """The H2 mechanisms with 2 or 4 cells per warp (16 or 8 lanes per cell):
-    the right-hand side is bitwise that of one cell per warp (same reaction
-    slots, same gather lists and order, same reduction trees), the integration
-    passes the parity gates against the CPU oracle in both precisions, and the
-    counters track the oracle's."""
-    b = W.make(wl, 333, seed=23)
-    s32 = native.Solver(mech, lanes_per_cell=32)
-    sg = native.Solver(mech, lanes_per_cell=lanes)
-    f32 = s32.eval_rhs(b.T, b.Y, b.P)
-    fg = sg.eval_rhs(b.T, b.Y, b.P)
-    s32.close()
-    sg.close()
-    assert np.array_equal(f32[0], fg[0]) and np.array_equal(f32[1], fg[1])
-    yo, so = oracle.bdf(b.mech, b.state_rows(), b.P, b.dt, rtol=W.RTOL, atol=W.ATOL, threads=8)
-    for precision in (native.B200ODE_FP64, native.B200ODE_MIXED):
-        T, Y, st, stats, cnt = run_gpu(b, precision, counters=True, lanes_per_cell=lanes)
-        assert (st == 0).all()
-        compare(b, T, Y, yo, f"{mech}/{lanes}/{precision}", oracle)
-        assert np.abs(Y.sum(axis=0) - 1.0).max() < 1e-12
-        for k in ("nst", "nni"):
-            g, c = cnt[k].sum(), so[k].sum()
-            assert abs(g - c) <= 0.1 * c + 10, (k, g, c)
-    # persistent == step form with several cells per warp
-    Tp, Yp, sp, _, _ = run_gpu(b, native.B200ODE_FP64, lanes_per_cell=lanes)
-    Ts, Ys, ss, _, _ = run_gpu(b, native.B200ODE_FP64, persistent=0, lanes_per_cell=lanes)
-    assert np.array_equal(Tp, Ts) and np.array_equal(Yp, Ys) and np.array_equal(sp, ss)
-
-
-def test_lanes_per_cell_is_validated():
-    with pytest.raises(native.B200Error):
-        native.Solver("gri30", lanes_per_cell=16)
-    with pytest.raises(native.B200Error):
-        native.Solver("h2o2", lanes_per_cell=12)
