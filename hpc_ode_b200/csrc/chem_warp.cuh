@@ -584,17 +584,34 @@ __device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off,
     for (int r = 0; r < LISTS; ++r) acc[r] = 0.0;
     const int gmax = M.gmax;
     const int* gw = M.gword + lane;
-#pragma unroll 2
-    for (int e = 0; e < gmax; ++e) {
+    // entries in batches of kE: the batch's words and source values are all
+    // loaded before any partial sum is stored (src and part are both shared
+    // memory, so a load may not pass a store and an unbatched loop would wait
+    // out the word and value load latencies once per entry); the sums see the
+    // same entries in the same order
+    constexpr int kE = 4;
+#pragma unroll 1
+    for (int e0 = 0; e0 < gmax; e0 += kE) {
 #pragma unroll
         for (int r = 0; r < LISTS; ++r) {   // lane's lists: lane, lane + G, ...
-            const int w = __ldg(gw + 32 * e + G * r);
-            double nu = (double)(((w >> 11) & 31) - 16);
-            if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
-            acc[r] += nu * src[w & 2047];
-            const bool last = (w >> 16) & 1;
-            if (last) sm->part[w >> 17] = acc[r];
-            acc[r] = last ? 0.0 : acc[r];
+            int w[kE];
+            double v[kE];
+#pragma unroll
+            for (int q = 0; q < kE; ++q) {
+                // past the end: a padding word (the last slot, an inactive one
+                // whose rate is 0; nu 0; not the last entry of a unit)
+                w[q] = (e0 + q < gmax) ? __ldg(gw + 32 * (e0 + q) + G * r) : ((MT::NSLOT - 1) | (16 << 11));
+                v[q] = src[w[q] & 2047];
+            }
+#pragma unroll
+            for (int q = 0; q < kE; ++q) {
+                double nu = (double)(((w[q] >> 11) & 31) - 16);
+                if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
+                acc[r] += nu * v[q];
+                const bool last = (w[q] >> 16) & 1;
+                if (last) sm->part[w[q] >> 17] = acc[r];
+                acc[r] = last ? 0.0 : acc[r];
+            }
         }
     }
     __syncwarp(gmask<G>());

@@ -245,6 +245,9 @@ __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off
     return sing;
 }
 
+// Matrices from this size up take the batched rank-1 update in the compact form.
+constexpr int kBatchedUpdateMinN = 32;
+
 // The unblocked right-looking form of the same factorization (row by row,
 // one rank-1 update per column): the smallest code.  With several warps per
 // SM the latency it exposes is hidden by the other warps, and the kernels of
@@ -293,15 +296,54 @@ __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off
         if (lane == 0) dinv[k] = inv;
         for (int i = k + 1 + lane; i < N; i += G) A[i * LDA + k] *= inv;
         __syncwarp(gm);
-        // rank-1 update of the trailing block; lane owns columns j.  (Batching
-        // each column's loads ahead of its stores measured neutral for GRI-Mech
-        // 3.0 and cost the 10-species mechanisms a third of their resident warps
-        // through the registers it takes, so the element-wise form stays.)
-        for (int j = k + 1 + lane; j < N; j += G) {
-            const LinT ukj = A[k * LDA + j];
-            if (ukj != LinT(0)) {
+        // rank-1 update of the trailing block; lane owns columns j = lane + G s > k.
+        if constexpr (N >= kBatchedUpdateMinN) {
+            // rows in batches of kRows whose multipliers and entries are all
+            // loaded before any store (a load may not pass a store to the same
+            // array, so element-by-element updates would each wait out the full
+            // shared-memory latency); every element gets the same single fused
+            // multiply-add as in the element-wise form below
+            constexpr int kRows = 8;
+            LinT u[NS];
+            bool on[NS];
+            bool any = false;
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int j = lane + G * s;
+                u[s] = (j > k && j < N) ? A[k * LDA + j] : LinT(0);
+                on[s] = u[s] != LinT(0);
+                any = any || on[s];
+            }
+            if (__any_sync(gm, any)) {
+#pragma unroll 1
+                for (int i0 = k + 1; i0 < N; i0 += kRows) {
+                    LinT l[kRows];
+#pragma unroll
+                    for (int r = 0; r < kRows; ++r) l[r] = (i0 + r < N) ? A[(i0 + r) * LDA + k] : LinT(0);
+#pragma unroll
+                    for (int s = 0; s < NS; ++s) {
+                        if (on[s]) {
+                            const int j = lane + G * s;
+                            LinT a[kRows];
+#pragma unroll
+                            for (int r = 0; r < kRows; ++r)
+                                if (i0 + r < N) a[r] = A[(i0 + r) * LDA + j];
+#pragma unroll
+                            for (int r = 0; r < kRows; ++r)
+                                if (i0 + r < N) A[(i0 + r) * LDA + j] = a[r] - l[r] * u[s];
+                        }
+                    }
+                }
+            }
+        } else {
+            // the smallest matrices: the short element-wise form (the batched one
+            // takes registers that cost these kernels resident warps)
+            for (int j = k + 1 + lane; j < N; j += G) {
+                const LinT ukj = A[k * LDA + j];
+                if (ukj != LinT(0)) {
 #pragma unroll 4
-                for (int i = k + 1; i < N; ++i) A[i * LDA + j] -= A[i * LDA + k] * ukj;
+                    for (int i = k + 1; i < N; ++i) A[i * LDA + j] -= A[i * LDA + k] * ukj;
+                }
             }
         }
         __syncwarp(gm);
@@ -348,26 +390,57 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
         x[s] = (i < N) ? (LinT)v : LinT(0);
     }
     // forward: unit lower (rolled: this runs every Newton iteration and must
-    // stay small in the instruction cache)
+    // stay small in the instruction cache).  Column k+1's entries are loaded
+    // while column k is applied, so the loop-carried chain is the broadcast of
+    // x_k and one fused multiply-add (A is not written here: the loads may run
+    // ahead of the arithmetic).
+    LinT col[NS];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int i = lane + G * s;
+        col[s] = (i > 0 && i < N) ? A[i * LDA + 0] : LinT(0);
+    }
 #pragma unroll 1
     for (int k = 0; k < N - 1; ++k) {
+        LinT nxt[NS];
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int i = lane + G * s;
+            nxt[s] = (i > k + 1 && i < N) ? A[i * LDA + k + 1] : LinT(0);
+        }
         const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + G * s;
-            if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
+            if (i > k && i < N) x[s] -= col[s] * xk;
+            col[s] = nxt[s];
         }
     }
-    // backward: upper
+    // backward: upper, with column k-1 and 1/U_{k-1,k-1} loaded ahead the same way
+    LinT dk = dinv[N - 1];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int i = lane + G * s;
+        col[s] = (i < N - 1) ? A[i * LDA + N - 1] : LinT(0);
+    }
 #pragma unroll 1
     for (int k = N - 1; k >= 0; --k) {
-        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dinv[k];
+        LinT nxt[NS];
+        const LinT dn = (k > 0) ? dinv[k - 1] : LinT(0);
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const int i = lane + G * s;
+            nxt[s] = (k > 0 && i < k - 1) ? A[i * LDA + k - 1] : LinT(0);
+        }
+        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dk;
         if (lane == (k % G)) place<NS>(x, k / G, xk);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + G * s;
-            if (i < k) x[s] -= A[i * LDA + k] * xk;
+            if (i < k) x[s] -= col[s] * xk;
+            col[s] = nxt[s];
         }
+        dk = dn;
     }
     // A species no reaction changes has a zero row in J, so its row of M is
     // the identity row and its solution component is exactly its right-hand
