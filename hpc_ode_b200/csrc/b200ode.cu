@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(128) k_eval_jac(const __grid_constant__ KParam
     Vec<MT::NS> y;
     load_cell<MT>(p, cell, lane, y.v);
     const double P = pressure_slot<MT>(p, cell, y.v, lane);
-    warp_jac<MT, LinT>(P, y, smem_off(sm->A), smem_off(&sm->chem), &wg->js, lane);
+    warp_jac<MT, LinT>(P, y, smem_off(sm->A), smem_off(&sm->chem), &wg->js, wg->savedJ, lane);
     constexpr int N = MT::N;
     double* out = jac + cell * (long long)(N * N);
     for (int i = 0; i < N; ++i)

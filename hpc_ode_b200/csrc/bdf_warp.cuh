@@ -84,7 +84,11 @@ struct WarpSmem {
 // without re-evaluating J) and the Jacobian's rate-derivative scratch.
 template <class MT, class LinT>
 struct WarpGlobal {
-    LinT savedJ[MT::N * MT::N];
+    // the saved Jacobian N x N; while a new Jacobian is evaluated (before it
+    // is saved here) the same space holds its per-slot derivative pieces
+    // [kJacPieces][NSLOT], so it is sized for the larger of the two
+    static constexpr int kSaved = (MT::N * MT::N > kJacPieces * MT::NSLOT) ? MT::N * MT::N : kJacPieces * MT::NSLOT;
+    LinT savedJ[kSaved];
     JacScratch<MT> js;
 };
 
@@ -314,7 +318,7 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
         S.nstlj = S.nst;
         S.jcur = 1;
         const long long tj = ph_tick(S);
-        warp_jac<MT, LinT>(S.P, yv, smem_off(A), smem_off(&w->chem), &wg->js, lane);
+        warp_jac<MT, LinT>(S.P, yv, smem_off(A), smem_off(&w->chem), &wg->js, wg->savedJ, lane);
         ph_tock(S, PH_JAC, tj, lane);
     }
 #pragma unroll 1

@@ -584,34 +584,17 @@ __device__ __noinline__ Vec<MT::NS> gather(const double* gsrc, unsigned src_off,
     for (int r = 0; r < LISTS; ++r) acc[r] = 0.0;
     const int gmax = M.gmax;
     const int* gw = M.gword + lane;
-    // entries in batches of kE: the batch's words and source values are all
-    // loaded before any partial sum is stored (src and part are both shared
-    // memory, so a load may not pass a store and an unbatched loop would wait
-    // out the word and value load latencies once per entry); the sums see the
-    // same entries in the same order
-    constexpr int kE = 4;
-#pragma unroll 1
-    for (int e0 = 0; e0 < gmax; e0 += kE) {
+#pragma unroll 2
+    for (int e = 0; e < gmax; ++e) {
 #pragma unroll
         for (int r = 0; r < LISTS; ++r) {   // lane's lists: lane, lane + G, ...
-            int w[kE];
-            double v[kE];
-#pragma unroll
-            for (int q = 0; q < kE; ++q) {
-                // past the end: a padding word (the last slot, an inactive one
-                // whose rate is 0; nu 0; not the last entry of a unit)
-                w[q] = (e0 + q < gmax) ? __ldg(gw + 32 * (e0 + q) + G * r) : ((MT::NSLOT - 1) | (16 << 11));
-                v[q] = src[w[q] & 2047];
-            }
-#pragma unroll
-            for (int q = 0; q < kE; ++q) {
-                double nu = (double)(((w[q] >> 11) & 31) - 16);
-                if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
-                acc[r] += nu * v[q];
-                const bool last = (w[q] >> 16) & 1;
-                if (last) sm->part[w[q] >> 17] = acc[r];
-                acc[r] = last ? 0.0 : acc[r];
-            }
+            const int w = __ldg(gw + 32 * e + G * r);
+            double nu = (double)(((w >> 11) & 31) - 16);
+            if constexpr (MT::NU_DEN != 1) nu *= 1.0 / MT::NU_DEN;   // exact: a power of two
+            acc[r] += nu * src[w & 2047];
+            const bool last = (w >> 16) & 1;
+            if (last) sm->part[w >> 17] = acc[r];
+            acc[r] = last ? 0.0 : acc[r];
         }
     }
     __syncwarp(gmask<G>());
@@ -698,11 +681,13 @@ __device__ __noinline__ Vec<MT::NS> warp_rhs(double P, const Vec<MT::NS> yv, uns
 // fixed) the second term is absent, C does not depend on T, and the total
 // concentration m = sum_i C_i (third bodies, PLOG pressure) adds
 // dw/dm (1/W_j - 1/W_{N-1}) rho to every column.
-// d q / d C_j is scattered into the species-space rows with shared-memory
-// atomics (one warp per cell, so the accumulation never leaves the warp).
+// Each reaction slot's derivative pieces (d q / d C of its reactant and product
+// factors and its third-body term) go to dpiece (global scratch: the space the
+// Jacobian is saved into afterwards); the species-space block is then summed
+// from them by the Jacobian gather, each output element by one lane.
 template <class MT, class LinT>
 __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A_off, unsigned chem_off,
-                                      JacScratch<MT>* js, int lane) {
+                                      JacScratch<MT>* js, LinT* dpiece, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
     static_assert(3 * N <= MT::NSLOT, "the per-species work [3][N] reuses the rate buffer q[NSLOT]");
     const unsigned gm = gmask<G>();
@@ -780,31 +765,38 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
         sm->q[s] = o.q;
         js->dqdT[s] = dqdT;
         js->sr[s] = sr;
-        if (fl & kFlagActive) {
-            const int off = __ldg(M.tb_off + s), len = __ldg(M.tb_len + s);
-            const int cat = (fl & kFlagCatalyst) ? __ldg(M.cat_sp + s) : -1;
-#pragma unroll 1
-            for (int e = 0; e < kJRow; ++e) {
-                const int k = __ldg(M.jrow + e * ns + s);
-                if (k < 0) break;
-                const double nu = __ldg(M.jnu + e * ns + s);
-                LinT* row = A + k * LDA;
+        // the slot's derivative pieces (every slot, inactive ones as 0, so the
+        // gather's padding entries read finite values)
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    if (rf[a] < N) atomicAdd(row + rf[a], (LinT)(nu * dRf[a]));
-                    if (pf[a] < N) atomicAdd(row + pf[a], (LinT)(-nu * dRr[a]));
-                }
-                const double tt = nu * thd_term;
-                if (cat >= 0) {
-                    // [M] = m - sum_{k != cat} C_k: d[M]/dC_j = -1 for j != cat
-#pragma unroll 1
-                    for (int j = 0; j < N; ++j)
-                        if (j != cat) atomicAdd(row + j, (LinT)(-tt));
-                } else {
-#pragma unroll 1
-                    for (int t = 0; t < len; ++t)
-                        atomicAdd(row + __ldg(M.tb_sp + off + t), (LinT)(tt * __ldg(M.tb_alpha + off + t)));
-                }
+        for (int a = 0; a < 3; ++a) {
+            dpiece[a * ns + s] = (LinT)dRf[a];
+            dpiece[(3 + a) * ns + s] = (LinT)dRr[a];
+        }
+        dpiece[6 * ns + s] = (LinT)thd_term;
+    }
+    __syncwarp(gm);
+    // species-space block d omega_k / d C_j = sum_r nu_kr d q_r / d C_j by the
+    // Jacobian gather (mech_dev.h): every output element is summed by one lane
+    // in a fixed order and stored once -- no atomics, no conflicts between
+    // lanes that share a row or column (a third-body reaction reaches a whole
+    // row; most reactions share H, O or OH), results independent of scheduling
+    {
+        constexpr int LISTS = 32 / G;
+        const int jgmax = M.jgmax;
+        double acc[LISTS];
+#pragma unroll
+        for (int r = 0; r < LISTS; ++r) acc[r] = 0.0;
+#pragma unroll 2
+        for (int e = 0; e < jgmax; ++e) {
+#pragma unroll
+            for (int r = 0; r < LISTS; ++r) {
+                const int x = 32 * e + lane + G * r;
+                const int w = __ldg(M.jword + x);
+                const double cf = __ldg(M.jcoef + x);
+                acc[r] += cf * (double)dpiece[((w >> 11) & 7) * ns + (w & 2047)];
+                const bool last = (w >> 14) & 1;
+                if (last) A[w >> 15] = (LinT)acc[r];
+                acc[r] = last ? 0.0 : acc[r];
             }
         }
     }

@@ -390,57 +390,27 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
         x[s] = (i < N) ? (LinT)v : LinT(0);
     }
     // forward: unit lower (rolled: this runs every Newton iteration and must
-    // stay small in the instruction cache).  Column k+1's entries are loaded
-    // while column k is applied, so the loop-carried chain is the broadcast of
-    // x_k and one fused multiply-add (A is not written here: the loads may run
-    // ahead of the arithmetic).
-    LinT col[NS];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int i = lane + G * s;
-        col[s] = (i > 0 && i < N) ? A[i * LDA + 0] : LinT(0);
-    }
+    // stay small in the instruction cache; loading the next column ahead of
+    // the current one measured slower)
 #pragma unroll 1
     for (int k = 0; k < N - 1; ++k) {
-        LinT nxt[NS];
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int i = lane + G * s;
-            nxt[s] = (i > k + 1 && i < N) ? A[i * LDA + k + 1] : LinT(0);
-        }
         const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + G * s;
-            if (i > k && i < N) x[s] -= col[s] * xk;
-            col[s] = nxt[s];
+            if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
         }
     }
-    // backward: upper, with column k-1 and 1/U_{k-1,k-1} loaded ahead the same way
-    LinT dk = dinv[N - 1];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        const int i = lane + G * s;
-        col[s] = (i < N - 1) ? A[i * LDA + N - 1] : LinT(0);
-    }
+    // backward: upper
 #pragma unroll 1
     for (int k = N - 1; k >= 0; --k) {
-        LinT nxt[NS];
-        const LinT dn = (k > 0) ? dinv[k - 1] : LinT(0);
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int i = lane + G * s;
-            nxt[s] = (k > 0 && i < k - 1) ? A[i * LDA + k - 1] : LinT(0);
-        }
-        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dk;
+        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dinv[k];
         if (lane == (k % G)) place<NS>(x, k / G, xk);
 #pragma unroll
         for (int s = 0; s < NS; ++s) {
             const int i = lane + G * s;
-            if (i < k) x[s] -= col[s] * xk;
-            col[s] = nxt[s];
+            if (i < k) x[s] -= A[i * LDA + k] * xk;
         }
-        dk = dn;
     }
     // A species no reaction changes has a zero row in J, so its row of M is
     // the identity row and its solution component is exactly its right-hand

@@ -19,6 +19,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -44,6 +45,19 @@ constexpr int kJRow = 8;
 //   bit  16    last entry of its unit   bits 17-31 unit index
 // (nu_den = 1, or 2 / 4 for mechanisms with fractional product coefficients).
 constexpr int kGatherUnit = 24;
+
+// Jacobian gather (the species-space block of the analytic Jacobian,
+// d omega_k / d C_j = sum over reactions r of nu_kr d q_r / d C_j): one list
+// entry per (output element (k, j), reaction slot, derivative piece), the
+// entries of each output element contiguous and in a fixed order, output
+// elements dealt longest-first to the 32 lists.  Entry word (int32):
+//   bits 0-10  reaction slot     bits 11-13 derivative piece (0-2: d(forward
+//   rate)/d(reactant factor a), 3-5: d(reverse rate)/d(product factor a), 6: the
+//   third-body term)     bit 14  last entry of its output element
+//   bits 15-31 output element k * LDA + j
+// with a double coefficient per entry (nu_kr, -nu_kr, nu_kr * alpha_j or
+// -nu_kr for a catalyst's "all other species").
+constexpr int kJacPieces = 7;
 
 // Pointers into one device allocation (all arrays contiguous).
 struct DevMech {
@@ -95,6 +109,9 @@ struct DevMech {
     const double* plog_b;
     const double* plog_EaR;
     const int* inert;       // [nsp] 1: no reaction changes species k (its rows of J are zero)
+    int jgmax;              // entries per list of the Jacobian gather
+    const int* jword;       // [jgmax][32] Jacobian gather words, list innermost
+    const double* jcoef;    // [jgmax][32] their coefficients
 };
 
 // Host image of DevMech: one byte buffer plus offsets, copied to the device once.
@@ -110,8 +127,10 @@ struct HostMech {
         o_EaR0, o_A0const, o_troe_a, o_troe_iT3, o_troe_iT1, o_troe_T2, o_flags, o_rf, o_pf,
         o_dnu, o_tb_off, o_tb_len, o_tb_sp, o_tb_alpha, o_jrow, o_jnu, o_sp_off, o_sp_slot,
         o_sp_nu, o_cat_sp, o_gword, o_unit_off, o_plog_lev0, o_plog_nlev, o_plog_lnP, o_plog_toff,
-        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert;
-    int gmax = 0, nunit = 0;
+        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert, o_jword, o_jcoef;
+    int gmax = 0, nunit = 0, jgmax = 0, njent = 0;
+    std::vector<int> jword;      // Jacobian gather (see kJacPieces), also kept for host checks
+    std::vector<double> jcoef;
 
     DevMech bind(const unsigned char* base) const {
         DevMech d;
@@ -160,6 +179,9 @@ struct HostMech {
         d.plog_b = (const double*)(base + o_plog_b);
         d.plog_EaR = (const double*)(base + o_plog_EaR);
         d.inert = (const int*)(base + o_inert);
+        d.jgmax = jgmax;
+        d.jword = (const int*)(base + o_jword);
+        d.jcoef = (const double*)(base + o_jcoef);
         return d;
     }
 };
@@ -378,6 +400,64 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
     if (ns > 2048 || (int)units.size() >= (1 << 15)) { *err = "mechanism too large for the gather encoding"; return HostMech(); }
     h.gmax = gmax;
     h.nunit = (int)units.size();
+    // ---- Jacobian gather: entries per output element (k, j) in slot order
+    {
+        const int lda = (n % 2 == 0) ? n + 1 : n;
+        struct JEnt { int slot, piece; double coef; };
+        std::map<int, std::vector<JEnt>> outs;   // output element -> entries
+        for (int s = 0; s < ns; ++s) {
+            if (h.slot_rxn[s] < 0) continue;
+            for (int e = 0; e < kJRow; ++e) {
+                const int k = jrow[e * ns + s];
+                if (k < 0) break;
+                const double nu = jnu[e * ns + s];
+                for (int a = 0; a < 3; ++a) {
+                    if (rf[a * ns + s] < n) outs[k * lda + rf[a * ns + s]].push_back({s, a, nu});
+                    if (pf[a * ns + s] < n) outs[k * lda + pf[a * ns + s]].push_back({s, 3 + a, -nu});
+                }
+                if (flags[s] & kFlagCatalyst) {
+                    for (int j = 0; j < n; ++j)
+                        if (j != catsp[s]) outs[k * lda + j].push_back({s, 6, -nu});
+                } else if ((flags[s] & kFlagTypeMask) != 0) {
+                    for (int t = tboff[s]; t < tboff[s] + tblen[s]; ++t)
+                        outs[k * lda + tbsp[t]].push_back({s, 6, nu * tbal[t]});
+                }
+            }
+        }
+        std::vector<std::pair<int, const std::vector<JEnt>*>> ol;
+        for (auto& kv : outs) ol.push_back({kv.first, &kv.second});
+        std::vector<int> oord(ol.size());
+        for (size_t i = 0; i < ol.size(); ++i) oord[i] = (int)i;
+        std::stable_sort(oord.begin(), oord.end(), [&](int a, int b2) { return ol[a].second->size() > ol[b2].second->size(); });
+        std::vector<std::vector<int>> lane_outs(32);
+        std::vector<int> jload(32, 0);
+        for (int o : oord) {   // longest-first onto the least-loaded list
+            int best = 0;
+            for (int l = 1; l < 32; ++l) if (jload[l] < jload[best]) best = l;
+            lane_outs[best].push_back(o);
+            jload[best] += (int)ol[o].second->size();
+        }
+        int jgmax = 1;
+        for (int l = 0; l < 32; ++l) jgmax = std::max(jgmax, jload[l]);
+        if ((long long)(n - 1) * lda + n - 1 >= (1LL << 17)) { *err = "mechanism too large for the Jacobian gather"; return HostMech(); }
+        h.jword.assign((size_t)jgmax * 32, (ns - 1) | (6 << 11));   // padding: inactive slot, coefficient 0
+        h.jcoef.assign((size_t)jgmax * 32, 0.0);
+        int nj = 0;
+        for (int l = 0; l < 32; ++l) {
+            int e = 0;
+            for (int o : lane_outs[l]) {
+                const auto& v = *ol[o].second;
+                for (size_t x = 0; x < v.size(); ++x, ++e) {
+                    const int last = (x + 1 == v.size()) ? 1 : 0;
+                    h.jword[(size_t)e * 32 + l] = v[x].slot | (v[x].piece << 11) | (last << 14) | (ol[o].first << 15);
+                    h.jcoef[(size_t)e * 32 + l] = v[x].coef;
+                    ++nj;
+                }
+            }
+        }
+        h.jgmax = jgmax;
+        h.njent = nj;
+    }
     if (spslot.empty()) { spslot.push_back(0); spnu.push_back(0); }
     h.nent = (int)spslot.size();
     // ---- species arrays
@@ -420,6 +500,8 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
     std::vector<int> inert(n);
     for (int k = 0; k < n; ++k) inert[k] = spoff[k + 1] == spoff[k];
     h.o_inert = PUTV(inert);
+    h.o_jword = PUTV(h.jword);
+    h.o_jcoef = PUTV(h.jcoef);
 #undef PUTV
     h.blob.resize((h.blob.size() + 255) & ~size_t(255));
     return h;

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdio>
 #include <map>
+#include <tuple>
 #include <string>
 #include <utility>
 #include <vector>
@@ -154,8 +155,62 @@ static int check(const GenTables& g, int nunits_generated, int nplog_generated) 
     for (int k = 0; k < n; ++k)
         if (unit_off[k] < 0 || unit_off[k + 1] < unit_off[k] || unit_off[k + 1] > h.nunit) return bad("species units", k, unit_off[k]);
     if (3 * n > ns) return bad("Jacobian per-species work [3][N] exceeds the rate buffer", ns, 3 * n);
-    std::printf("ok %s nslot %d nunit %d gmax %d plog %d inert %d nu_den %d (indices in range)\n", g.name, ns, h.nunit,
-                h.gmax, nplog, ninert, g.nu_den);
+    // the Jacobian gather: its (output element, slot, piece) -> coefficient map
+    // equals the scatter the tables describe -- for each net-stoichiometry row k
+    // of each slot: +nu at (k, reactant factor a) piece a, -nu at (k, product
+    // factor a) piece 3 + a, and at (k, j) piece 6: nu * alpha_j for the
+    // third-body species j, or -nu for every j but the catalyst; every output
+    // element is written exactly once, by its last entry
+    {
+        const int lda = (n % 2 == 0) ? n + 1 : n;
+        std::map<std::tuple<int, int, int>, double> jwant, jgot;
+        const double* jnu = at<double>(h, h.o_jnu);
+        const double* tb_al = at<double>(h, h.o_tb_alpha);
+        for (int s = 0; s < ns; ++s) {
+            if (h.slot_rxn[s] < 0) continue;
+            for (int e = 0; e < b200::kJRow; ++e) {
+                const int k = jrow[e * ns + s];
+                if (k < 0) break;
+                const double nu = jnu[e * ns + s];
+                for (int a = 0; a < 3; ++a) {
+                    if (rf[a * ns + s] < n) jwant[{k * lda + rf[a * ns + s], s, a}] += nu;
+                    if (pf[a * ns + s] < n) jwant[{k * lda + pf[a * ns + s], s, 3 + a}] += -nu;
+                }
+                if (flags[s] & b200::kFlagCatalyst) {
+                    for (int j = 0; j < n; ++j) if (j != cat_sp[s]) jwant[{k * lda + j, s, 6}] += -nu;
+                } else if (flags[s] & b200::kFlagTypeMask) {
+                    for (int t = tb_off[s]; t < tb_off[s] + tb_len[s]; ++t) jwant[{k * lda + tb_sp[t], s, 6}] += nu * tb_al[t];
+                }
+            }
+        }
+        const int* jw = at<int>(h, h.o_jword);
+        const double* jc = at<double>(h, h.o_jcoef);
+        std::map<int, int> written;
+        for (int l = 0; l < 32; ++l) {
+            int cur = -1;
+            for (int e = 0; e < h.jgmax; ++e) {
+                const int w = jw[e * 32 + l];
+                const int slot = w & 2047, piece = (w >> 11) & 7, last = (w >> 14) & 1, out = w >> 15;
+                if (slot >= ns || piece >= b200::kJacPieces) return bad("Jacobian gather word", e, w);
+                if (jc[e * 32 + l] == 0.0 && !last && h.slot_rxn[slot] < 0) continue;   // padding
+                if (out >= n * lda || out % lda >= n) return bad("Jacobian gather output", e, out);
+                if (cur >= 0 && out != cur) return bad("Jacobian gather unit not contiguous", e, out);
+                cur = out;
+                jgot[{out, slot, piece}] += jc[e * 32 + l];
+                if (last) { written[out] += 1; cur = -1; }
+            }
+            if (cur >= 0) return bad("Jacobian gather unit without a last entry", l, cur);
+        }
+        if (jgot.size() != jwant.size()) return bad("Jacobian gather entry count", (int)jgot.size(), (int)jwant.size());
+        for (const auto& kv : jwant) {
+            auto it = jgot.find(kv.first);
+            if (it == jgot.end() || std::fabs(it->second - kv.second) > 1e-12 * (1.0 + std::fabs(kv.second)))
+                return bad("Jacobian gather coefficient", std::get<1>(kv.first), std::get<0>(kv.first));
+        }
+        for (const auto& kv : written) if (kv.second != 1) return bad("Jacobian output written twice", kv.first, kv.second);
+    }
+    std::printf("ok %s nslot %d nunit %d gmax %d plog %d inert %d nu_den %d jac entries %d jgmax %d (indices in range)\n",
+                g.name, ns, h.nunit, h.gmax, nplog, ninert, g.nu_den, h.njent, h.jgmax);
     return 0;
 }
 
