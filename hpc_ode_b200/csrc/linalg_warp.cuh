@@ -272,13 +272,26 @@ __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off
             const LinT v = absT(A[i * LDA + k]);
             if (v > best) { best = v; bi = i; }
         }
+        if constexpr (sizeof(LinT) == 4) {
+            // FP32: two warp reductions instead of a shuffle tree.  The bits of
+            // a non-negative float order as the floats do (the sign bit cleared:
+            // M holds -0.0 wherever gamma scaled a zero of J); key 0 = no
+            // candidate on this lane (none, or only NaN), so a key <= 1 means no
+            // pivot > 0.
+            const unsigned key = (best >= LinT(0)) ? __float_as_uint(fabsf((float)best)) + 1u : 0u;
+            const unsigned kmax = __reduce_max_sync(gm, key);
+            if (kmax <= 1u) { sing = k + 1; break; }   // zero (or NaN) pivot
+            // first index of the maximum: the smallest row among the lanes holding it
+            bi = (int)__reduce_min_sync(gm, key == kmax ? (unsigned)bi : (unsigned)N);
+        } else {
 #pragma unroll
-        for (int o = G / 2; o > 0; o >>= 1) {
-            const LinT ov = __shfl_xor_sync(gm, best, o, G);
-            const int oi = __shfl_xor_sync(gm, bi, o, G);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            for (int o = G / 2; o > 0; o >>= 1) {
+                const LinT ov = __shfl_xor_sync(gm, best, o, G);
+                const int oi = __shfl_xor_sync(gm, bi, o, G);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
         }
-        if (!(best > LinT(0))) { sing = k + 1; break; }   // zero (or NaN) pivot
         if (bi != k) {
 #pragma unroll 1
             for (int j = lane; j < N; j += G) {
