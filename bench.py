@@ -51,13 +51,24 @@ from hpc_ode_b200 import shard, workloads as W  # noqa: E402
 
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per cell of one k_bdf launch, from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum, 8,192-cell GRI capture, mixed precision): the traffic
-# is the compulsory T/P/Y in + T/Y/status out, so it scales with the cell count.
-NCU_DRAM_BYTES_PER_CELL = {"gri30": 789.0}
-# Warp instructions per cell-step of the same capture (smsp__inst_executed.sum /
-# (cells x BDF steps per cell), 8,192 GRI cells, mixed): scaled by the run's own
-# step count, issued instructions against the SMs' peak issue rate.
-NCU_WARP_INSTR_PER_CELL_STEP = {("gri30", "mixed"): 3.269e6 / 132.3}
+# dram__bytes_write.sum of one mixed-precision capture, divided by its cells):
+# the traffic is the compulsory T/P/Y in + T/Y/status out plus the mechanism
+# tables once, so it scales with the cell count (the kerosene capture, one cell
+# per SM, is table-dominated and is not scaled).  Values: (bytes, summary file).
+NCU_DRAM_BYTES_PER_CELL = {
+    "gri30": (762.0, "profiles/k_bdf_gri8k_mixed_full.txt"),
+    "h2o2": (114.0, "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    "nDodecane_Reitz": (2760.0, "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
+}
+# Warp instructions per cell-step of the same captures (smsp__inst_executed.sum /
+# (cells x BDF steps per cell)): scaled by the run's own step count, issued
+# instructions against the SMs' peak issue rate.
+NCU_WARP_INSTR_PER_CELL_STEP = {
+    ("gri30", "mixed"): (25.246e9 / (8192 * 132.98), "profiles/k_bdf_gri8k_mixed_full.txt"),
+    ("h2o2", "mixed"): (118.10e9 / (32768 * 558.06), "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    ("nDodecane_Reitz", "mixed"): (22.379e9 / (1024 * 551.23), "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
+    (W.ESTIMATE, "mixed"): (29.014e9 / (148 * 662.09), "profiles/k_bdf_kero148_mixed_sections.txt"),
+}
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 CPU_SAMPLE = {"gri_1m": 4096, "gri_bimodal": 8192, "gri_32k": 8192, "h2_1024": 1024, "h2li_grid": 4096,
               "nc12_8k": 512, "kero_2k": 64}
@@ -509,19 +520,19 @@ def main():
         roofline = {"bound": "fp64+fp32", "error": str(e)}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     alg_bytes = n * ((nsp + 1) * 8 + 8) + n * ((nsp + 1) * 8 + 4)   # T,Y,P in; T,Y,status out
-    per_cell = NCU_DRAM_BYTES_PER_CELL.get(batch.mech)
+    per_cell, dram_src = NCU_DRAM_BYTES_PER_CELL.get(batch.mech, (None, None))
     traffic = per_cell * n if per_cell else None
     roofline["traffic"] = traffic
     roofline["hbm"] = {"achieved_gbs": alg_bytes / (kernel_ms * 1e-3) / 1e9, "peak_gbs": hbm_peak,
                        "frac": alg_bytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, "alg_bytes": alg_bytes,
                        "traffic_bytes": traffic,
-                       "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 8,192-cell "
-                                          "k_bdf launch (profiles/k_bdf_gri8k_mixed_full.txt), scaled by cells"
+                       "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_bdf "
+                                          "launch (%s), per cell, scaled by cells" % dram_src
                                           if per_cell else None),
                        "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks
                                        else "fallback 6,650 GB/s (MEASURED_PEAKS.json absent)")}
     issue = None
-    ipcs = NCU_WARP_INSTR_PER_CELL_STEP.get((batch.mech, args.precision))
+    ipcs, ipcs_src = NCU_WARP_INSTR_PER_CELL_STEP.get((batch.mech, args.precision), (None, None))
     if ipcs and st:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         mhz = clk.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
@@ -529,8 +540,8 @@ def main():
         ach = ipcs * st["total_nst"] / (kernel_ms * 1e-3)
         issue = {"achieved_warp_inst_per_s": ach, "peak_warp_inst_per_s": peak_issue, "frac": ach / peak_issue,
                  "source": "warp instructions per cell-step from ncu smsp__inst_executed.sum "
-                           "(profiles/k_bdf_gri8k_mixed_full.txt) x this run's BDF steps / CUDA-event kernel "
-                           "time; peak = 4 schedulers x SMs x median SM clock"}
+                           "(%s) x this run's BDF steps / CUDA-event kernel "
+                           "time; peak = 4 schedulers x SMs x median SM clock" % ipcs_src}
 
     # ---- the plain FP64 one-launch-per-step form on the same cells (the
     # comparison the mixed persistent form is measured against); one GPU only
