@@ -158,7 +158,7 @@ def cpu_reference(batch: W.Batch, ncells: int, threads: int, conv: bool = False)
     return len(idx), el, kind, what, st
 
 
-def cpu_baseline_block(batch: W.Batch, sample: int, conv: bool = False, passes: int = 3) -> dict:
+def cpu_baseline_block(batch: W.Batch, sample: int, conv: bool = False, passes: int = 5) -> dict:
     """The CPU integrator on the host cores: OpenMP over all cores (schedule
     dynamic, 1; the reference's CVodeIntegratorOMP) as the baseline value, and
     serial (one core; the reference's CVodeIntegrator) beside it.  Each a
@@ -408,6 +408,12 @@ def main():
         batch = W.make(args.workload, args.ncells or cfg["ncells"], seed=cfg["seed"] + 1000 * rank)
         total_cells = ws * batch.ncells
     n = batch.ncells
+    # the CPU baseline first, in a process that has not yet touched the GPU
+    # (as the reference arm's process)
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_block(batch, args.cpu_sample or CPU_SAMPLE.get(args.workload, 4096),
+                                 conv=args.formulation == "conv")
     prec = native.B200ODE_MIXED if args.precision == "mixed" else native.B200ODE_FP64
     form = native.B200ODE_CONV if args.formulation == "conv" else native.B200ODE_CONP
     solver = native.Solver(batch.mech, precision=prec, persistent=int(args.form == "persistent"),
@@ -593,11 +599,6 @@ def main():
                                  conv=args.formulation == "conv")
         except Exception as e:  # noqa: BLE001
             acc = {"error": str(e)}
-
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_block(batch, args.cpu_sample or CPU_SAMPLE.get(args.workload, 4096),
-                                 conv=args.formulation == "conv")
 
     line = {
         "metric": "cells_per_sec", "value": value, "unit": "cells/s", "n_gpus": ws,

@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
     const bool step_form = p.records != nullptr;
     auto* wglob = reinterpret_cast<WarpGlobal<MT, LinT>*>(p.wglobal);
     const int profiling = (p.prof != nullptr && !step_form) ? 1 : 0;
-    if (lane < 8) S.prof[lane] = 0;
+    if (profiling && lane < 8) wglob[gw].prof[lane] = 0;
     __syncwarp(gmask<G>());
     const long long t_start = profiling ? clock64() : 0;
     unsigned long long tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         S.qmax = p.max_order;
         S.refine = p.refine;
         S.profiling = profiling;
+        S.prof = wg->prof;
         S.lu_dirty = 0;
         int status = 0;
         bool done = false;
@@ -378,8 +379,9 @@ __global__ void __launch_bounds__(128, MINB) k_bdf(const __grid_constant__ KPara
         for (int i = 0; i < 8; ++i)
             if (tot[i]) atomicAdd(p.totals + i, tot[i]);
     if (profiling && lane == 0) {
-        S.prof[PH_TOTAL] = clock64() - t_start;
-        for (int i = 0; i < 5; ++i) atomicAdd(p.prof + i, (unsigned long long)S.prof[i]);
+        long long* pr = wglob[gw].prof;
+        pr[PH_TOTAL] = clock64() - t_start;
+        for (int i = 0; i < 5; ++i) atomicAdd(p.prof + i, (unsigned long long)pr[i]);
     }
 }
 
@@ -515,24 +517,40 @@ b200ode_status ensure_wg(b200ode_handle* h, size_t bytes) {
     return B200ODE_OK;
 }
 
-// Warps per CTA: the option when set, else the shape (4, 2 or 1 warps per CTA)
-// that keeps the most warps resident per SM for this mechanism and precision
-// (shared memory per warp and registers decide), ties to the larger CTA.
-// Computed once per handle.
+// Threads per CTA of the BDF kernel for wpb cells per CTA: one 128-thread CTA
+// per cell when a widest mechanism's helper warps serve (wpb = 1).
+template <class MT>
+int bdf_threads(const b200ode_handle* h, int wpb) {
+    if (MT::N >= kWideN && wpb == 1 && h->opt.cta_helpers) return 32 * (kHelperWarps + 1);
+    return wpb * 32;
+}
+
+// Resident CTAs per SM of the BDF kernel's register variant MINB (launch
+// bounds of 1 or 3 CTAs per SM) at wpb warps per CTA; 0 if it does not fit.
+template <class MT, class LinT, int MINB>
+int bdf_occupancy(const b200ode_handle* h, int wpb) {
+    const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
+    auto k = k_bdf<MT, LinT, MINB>;
+    int bps = 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, bdf_threads<MT>(h, wpb), smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return bps;
+}
+
+// Warps per CTA: the option when set, else the shape (4, 2 or 1 warps per CTA,
+// either register variant) that keeps the most warps resident per SM for this
+// mechanism and precision (shared memory per warp and registers decide), ties
+// to the larger CTA.  Computed once per handle.
 template <class MT, class LinT>
 int pick_wpb(b200ode_handle* h) {
     if (h->opt.warps_per_block > 0) return std::min(h->opt.warps_per_block, 4);
     if (h->auto_wpb > 0) return h->auto_wpb;
     int best = 4, best_warps = -1;
     for (int wpb : {4, 2, 1}) {
-        const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
-        auto k = k_bdf<MT, LinT, 1>;
-        int bps = 0;
-        if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, wpb * 32, smem) != cudaSuccess) {
-            cudaGetLastError();
-            continue;
-        }
+        const int bps = std::max(bdf_occupancy<MT, LinT, 1>(h, wpb), bdf_occupancy<MT, LinT, 3>(h, wpb));
         if (bps * wpb > best_warps) {
             best_warps = bps * wpb;
             best = wpb;
@@ -542,12 +560,22 @@ int pick_wpb(b200ode_handle* h) {
     return best;
 }
 
-// Threads per CTA of the BDF kernel for wpb cells per CTA: one 128-thread CTA
-// per cell when a widest mechanism's helper warps serve (wpb = 1).
-template <class MT>
-int bdf_threads(const b200ode_handle* h, int wpb) {
-    if (MT::N >= kWideN && wpb == 1 && h->opt.cta_helpers) return 32 * (kHelperWarps + 1);
-    return wpb * 32;
+// The BDF kernel's register variant for wpb warps per CTA: launch bounds of 3
+// CTAs per SM (at most 168 registers a thread) when options.blocks_per_sm asks
+// for that many CTAs, or, with blocks_per_sm = 0, when that variant keeps more
+// CTAs resident than the unconstrained one (decided once per handle and CTA
+// shape; ties keep the unconstrained variant).
+template <class MT, class LinT>
+auto bdf_kernel(b200ode_handle* h, int wpb) -> void (*)(KParams) {
+    if (h->opt.blocks_per_sm > 0)
+        return h->opt.blocks_per_sm >= 3 * (4 / wpb) ? k_bdf<MT, LinT, 3> : k_bdf<MT, LinT, 1>;
+    const int key = wpb * 1024 + bdf_threads<MT>(h, wpb);
+    auto it = h->auto_minb.find(key);
+    if (it == h->auto_minb.end()) {
+        const bool v3 = bdf_occupancy<MT, LinT, 3>(h, wpb) > bdf_occupancy<MT, LinT, 1>(h, wpb);
+        it = h->auto_minb.emplace(key, v3 ? 3 : 1).first;
+    }
+    return it->second == 3 ? k_bdf<MT, LinT, 3> : k_bdf<MT, LinT, 1>;
 }
 
 template <class MT, class LinT>
@@ -555,8 +583,7 @@ b200ode_status launch_bdf(b200ode_handle* h, KParams& p, cudaStream_t st, int* l
     using R = StepRecord<MT, LinT>;
     const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
-    auto kern = k_bdf<MT, LinT, 1>;
-    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
+    auto kern = bdf_kernel<MT, LinT>(h, wpb);
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const size_t n = (size_t)p.ncells;
     CUDA_TRY(cudaMemsetAsync(h->d_ctl, 0, 16 * sizeof(unsigned long long), st));
@@ -662,8 +689,7 @@ b200ode_status persistent_shape(b200ode_handle* h, long long n, void (**kern)(KP
                                 int* wpb_out, size_t* smem_out) {
     const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
-    auto k = k_bdf<MT, LinT, 1>;
-    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) k = k_bdf<MT, LinT, 3>;
+    auto k = bdf_kernel<MT, LinT>(h, wpb);
     CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int bps = 0;
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k, bdf_threads<MT>(h, wpb), smem));
@@ -1233,9 +1259,11 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
     if (n <= 0 || !dT || !dY) return fail(B200ODE_ERR_INVALID, "autotune needs cells (device T and Y)");
     if (!dP && !(Ps > 0.0)) return fail(B200ODE_ERR_INVALID, "pressure must be > 0");
     const bool wide_mech = (h->mech == MECH_ESTIMATE);   // one cell per SM: helper warps on or off
-    // the sample: the first m cells (a few per SM for the widest mechanism, whose
-    // cells take seconds), copied so the caller's buffers stay untouched
-    const int64_t m = std::min<int64_t>(n, wide_mech ? 2 * (int64_t)h->num_sms : 8192);
+    // the sample: the first m cells -- 192 per SM, about 16 per resident warp, so
+    // that the timing reflects the work queue's steady state rather than its
+    // tail (two per SM for the widest mechanism, whose cells take seconds) --
+    // copied so the caller's buffers stay untouched
+    const int64_t m = std::min<int64_t>(n, (wide_mech ? 2 : 192) * (int64_t)h->num_sms);
     const size_t nsp = h->hm.nsp;
     rc = ensure_cap(h, (size_t)m);
     if (rc != B200ODE_OK) return rc;
@@ -1476,8 +1504,7 @@ b200ode_status launch_bdf_noalloc(b200ode_handle* h, KParams& p, unsigned char* 
     using WG = WarpGlobal<MT, LinT>;
     const int wpb = pick_wpb<MT, LinT>(h);
     const size_t smem = warp_smem_bytes<MT, LinT>() * wpb;
-    auto kern = k_bdf<MT, LinT, 1>;
-    if (h->opt.blocks_per_sm >= 3 * (4 / wpb)) kern = k_bdf<MT, LinT, 3>;
+    auto kern = bdf_kernel<MT, LinT>(h, wpb);
     CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const int threads = bdf_threads<MT>(h, wpb);
     int bps = 0;

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <map>
 #include <string>
 
 #include "../../include/b200ode.h"
@@ -34,6 +35,7 @@ struct b200ode_handle {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int last_blocks_per_sm = 0;
     int auto_wpb = 0;                        // warps per CTA picked by occupancy (0 = not yet)
+    std::map<int, int> auto_minb;            // register variant per CTA shape (see bdf_kernel)
 };
 
 namespace b200 {

@@ -66,7 +66,7 @@ struct BdfState {
     int q, qprime, qwait, L, indx_acor, jcur, convfail;
     int nst, nstlp, nstlj, nstloc, max_steps, qmax, refine, lu_dirty, profiling;
     int cnt[7];
-    long long prof[8];   // per-phase clock64 totals when profiling
+    long long* prof;     // per-phase clock64 totals when profiling (the warp's WarpGlobal::prof)
 };
 
 // Per-warp shared memory.
@@ -76,8 +76,8 @@ struct WarpSmem {
     double zn[cv::QMAX + 1][MT::G * MT::NS];   // Nordsieck history zn[j][i]
     BdfState st;
     LinT A[MT::N * MT::LDA];                // Jacobian, then the LU factors of M = I - gamma J
-    LinT dinv[MT::N];
-    int perm[MT::N];
+                                            // (diagonal: 1 / U_kk)
+    unsigned char perm[MT::N];              // row permutation of the factors
 };
 
 // Per-warp global scratch: saved Jacobian (CVODE keeps it to form new M
@@ -90,6 +90,7 @@ struct WarpGlobal {
     static constexpr int kSaved = (MT::N * MT::N > kJacPieces * MT::NSLOT) ? MT::N * MT::N : kJacPieces * MT::NSLOT;
     LinT savedJ[kSaved];
     JacScratch<MT> js;
+    long long prof[8];   // per-phase clock64 totals when profiling
 };
 
 template <class MT, class LinT>
@@ -347,7 +348,7 @@ __device__ __noinline__ int bdf_ls_setup(unsigned off, const Vec<MT::NS> yv, War
     __syncwarp(gmask<MT::G>());
     S.lu_dirty = 1;
     const long long tl = ph_tick(S);
-    const int r = warp_lu<MT, LinT>(smem_off(A), smem_off(w->perm), smem_off(w->dinv), lane);
+    const int r = warp_lu<MT, LinT>(smem_off(A), smem_off(w->perm), lane);
     ph_tock(S, PH_LU, tl, lane);
     S.cnt[C_NSETUPS]++;
     S.gamrat = 1.0;
@@ -369,7 +370,7 @@ __device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], con
     Vec<NS> a;
 #pragma unroll
     for (int s = 0; s < NS; ++s) a.v[s] = b[s];
-    Vec<NS> x = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), smem_off(w->dinv), a, lane);
+    Vec<NS> x = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), a, lane);
     if (S.refine && sizeof(LinT) < sizeof(double)) {
         // r = b - (I - gammap J) x in FP64; x += M^{-1} r
         Vec<NS> r;
@@ -386,7 +387,7 @@ __device__ __forceinline__ void bdf_solve(unsigned off, double (&b)[MT::NS], con
             }
             if (i < N) r.v[s] += S.gammap * acc;
         }
-        const Vec<NS> d = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), smem_off(w->dinv), r, lane);
+        const Vec<NS> d = warp_lu_solve<MT, LinT>(smem_off(w->A), smem_off(w->perm), r, lane);
 #pragma unroll
         for (int s = 0; s < NS; ++s) x.v[s] += d.v[s];
     }
@@ -785,7 +786,7 @@ struct StepRecord {
     static constexpr int N = MT::N;
     static constexpr size_t kStateBytes = (sizeof(BdfState) + 255) & ~size_t(255);
     static constexpr size_t kZnBytes = ((cv::QMAX + 1) * N * sizeof(double) + 255) & ~size_t(255);
-    static constexpr size_t kLuBytes = ((N * MT::LDA + N) * sizeof(LinT) + N * sizeof(int) + 255) & ~size_t(255);
+    static constexpr size_t kLuBytes = (N * MT::LDA * sizeof(LinT) + N * sizeof(int) + 255) & ~size_t(255);
     static constexpr size_t kBytes = kStateBytes + 8 + kZnBytes + kLuBytes;   // + phase word
     static constexpr size_t kPhaseOff = kStateBytes;
 };
@@ -810,9 +811,7 @@ __device__ __noinline__ void bdf_save(unsigned off, unsigned char* rec, int phas
         LinT* Ag = reinterpret_cast<LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
         for (int e = lane; e < N * MT::LDA; e += MT::G) Ag[e] = w->A[e];
-        #pragma unroll 1
-        for (int e = lane; e < N; e += MT::G) Ag[N * MT::LDA + e] = w->dinv[e];
-        int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA + N);
+        int* pg = reinterpret_cast<int*>(Ag + N * MT::LDA);
         #pragma unroll 1
         for (int e = lane; e < N; e += MT::G) pg[e] = w->perm[e];
     }
@@ -837,11 +836,9 @@ __device__ __noinline__ void bdf_load(unsigned off, const unsigned char* rec, in
     const LinT* Ag = reinterpret_cast<const LinT*>(rec + R::kStateBytes + 8 + R::kZnBytes);
 #pragma unroll 1
     for (int e = lane; e < N * MT::LDA; e += MT::G) w->A[e] = Ag[e];
+    const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA);
     #pragma unroll 1
-    for (int e = lane; e < N; e += MT::G) w->dinv[e] = Ag[N * MT::LDA + e];
-    const int* pg = reinterpret_cast<const int*>(Ag + N * MT::LDA + N);
-    #pragma unroll 1
-    for (int e = lane; e < N; e += MT::G) w->perm[e] = pg[e];
+    for (int e = lane; e < N; e += MT::G) w->perm[e] = (unsigned char)pg[e];
     __syncwarp(gmask<MT::G>());
 }
 

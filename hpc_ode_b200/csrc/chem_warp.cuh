@@ -143,7 +143,6 @@ template <class MT>
 struct ChemSmem {
     double C[MT::N + 1];          // concentrations [kmol/m^3]; C[N] = 1 (padding factor)
     double G[MT::N + 1];          // s/R - h/RT; G[N] = 0
-    double H[MT::N + 1];          // h/RT; H[N] = 0
     double q[MT::NSLOT];          // rates of progress (Jacobian: reused for per-species work)
     double part[MT::NUNITMAX];    // gather partial sums
 };
@@ -153,6 +152,7 @@ template <class MT>
 struct JacScratch {
     double dqdT[MT::NSLOT];       // d q / d T at fixed mass fractions
     double sr[MT::NSLOT];         // sum_i (d q / d C_i) C_i
+    double H[MT::N + 1];          // h/RT of every species (H[N] = 0)
 };
 
 // NASA-7 polynomials of species k at T: cp/R, h/RT, s/R - h/RT, d(cp/R)/dT.
@@ -178,6 +178,16 @@ struct CellThermo {
 // by instruction fetch (its hot code is larger than the SM's instruction
 // cache), so every call site that is not a full inline expansion helps.
 __device__ __noinline__ double ode_exp(double x) { return exp(x); }
+// Two independent exponentials in one call, so that their dependency chains
+// overlap (same function, same results as two ode_exp calls).  Taken by the
+// mechanisms of kPairedExpMinN unknowns up; the smaller ones' kernels are bound
+// by instruction fetch and registers, where the second copy of exp costs more
+// than the overlap saves.
+struct Exp2 {
+    double a, b;
+};
+__device__ __noinline__ Exp2 ode_exp2(double x, double y) { return Exp2{exp(x), exp(y)}; }
+constexpr int kPairedExpMinN = 64;
 __device__ __noinline__ double ode_log10(double x) { return log10(x); }
 __device__ __noinline__ double ode_log(double x) { return log(x); }
 __device__ __noinline__ double ode_exp10(double x) { return exp10(x); }
@@ -186,12 +196,13 @@ __device__ __noinline__ double ode_pow(double x, double y) { return pow(x, y); }
 // the scalar step-control code calls this single copy instead.
 __device__ __noinline__ double ode_div(double a, double b) { return a / b; }
 
-// Species phase: concentrations and Gibbs terms into shared memory.
+// Species phase: concentrations and Gibbs terms into shared memory; with a
+// non-null H (the Jacobian), h/RT of every species into H as well.
 template <class MT>
 __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, const double (&y)[MT::NS],
                                                     ChemSmem<MT>* sm, int lane, double (&Yk)[MT::NS],
                                                     double (&cpR)[MT::NS], double (&hRT)[MT::NS],
-                                                    double (&dcpR)[MT::NS]) {
+                                                    double (&dcpR)[MT::NS], double* H = nullptr) {
     constexpr int N = MT::N, G = MT::G;
     CellThermo c;
     c.T = group_shfl<G>(y[(N - 1) / G], (N - 1) % G);
@@ -232,7 +243,7 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
             csum += Ci;
             sm->C[i] = Ci;
             sm->G[i] = g;
-            sm->H[i] = hRT[s];
+            if (H) H[i] = hRT[s];
         } else {
             cpR[s] = hRT[s] = dcpR[s] = 0.0;
         }
@@ -241,8 +252,9 @@ __device__ __forceinline__ CellThermo species_phase(const DevMech& M, double P, 
     if (lane == 0) {
         sm->C[N] = 1.0;
         sm->G[N] = 0.0;
-        sm->H[N] = 0.0;
+        if (H) H[N] = 0.0;
     }
+    if (H) __threadfence_block();   // H is global: order it for the other lanes
     __syncwarp(gmask<G>());
     return c;
 }
@@ -280,7 +292,15 @@ __device__ __noinline__ FallOut falloff(int s, int fl, double T, double logT, do
     double F = 1.0, dl_dx = 0.0, dl_dT = 0.0;
     if (type == 3) {
         const double a = __ldg(M.troe_a + s), iT3 = __ldg(M.troe_iT3 + s), iT1 = __ldg(M.troe_iT1 + s);
-        const double e3 = ode_exp(-c.T * iT3), e1 = ode_exp(-c.T * iT1);
+        double e3, e1;
+        if constexpr (MT::N >= kPairedExpMinN) {
+            const Exp2 e31 = ode_exp2(-c.T * iT3, -c.T * iT1);
+            e3 = e31.a;
+            e1 = e31.b;
+        } else {
+            e3 = ode_exp(-c.T * iT3);
+            e1 = ode_exp(-c.T * iT1);
+        }
         double Fcent = (1.0 - a) * e3 + a * e1;
         double dFcent = 0.0;
         if (Deriv) dFcent = -(1.0 - a) * iT3 * e3 - a * iT1 * e1;
@@ -395,18 +415,29 @@ __device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, u
             o.dlnkf_dT = pl.dlnk_dT;
         }
     }
-    const double kf = (fl & kFlagConstK) ? __ldg(M.Aconst + s) : ode_exp(lkf);
-    o.kf = kf;
-    o.Rf = kf * ((C[r0] * C[r1]) * C[r2]);
+    const bool constk = fl & kFlagConstK;
+    double kf;
     if (fl & kFlagRev) {
         const int p0 = __ldg(M.pf + s), p1 = __ldg(M.pf + ns + s), p2 = __ldg(M.pf + 2 * ns + s);
         const int dnu = __ldg(M.dnu + s);
         const double sg = (G[p0] + G[p1] + G[p2]) - (G[r0] + G[r1] + G[r2]);
         const double lnKc = sg - dnu * c.logT + __ldg(M.lnPfac + s);
-        const double kr = (fl & kFlagConstK) ? __ldg(M.Aconst + s) * ode_exp(-lnKc) : ode_exp(lkf - lnKc);
+        double kr;
+        if constexpr (MT::N >= kPairedExpMinN) {   // kf's and kr's exponentials in one call
+            const Exp2 e = ode_exp2(lkf, constk ? -lnKc : lkf - lnKc);
+            kf = constk ? __ldg(M.Aconst + s) : e.a;
+            kr = constk ? __ldg(M.Aconst + s) * e.b : e.b;
+        } else {
+            kf = constk ? __ldg(M.Aconst + s) : ode_exp(lkf);
+            kr = constk ? __ldg(M.Aconst + s) * ode_exp(-lnKc) : ode_exp(lkf - lnKc);
+        }
         o.kr = kr;
         o.Rr = kr * ((C[p0] * C[p1]) * C[p2]);
+    } else {
+        kf = constk ? __ldg(M.Aconst + s) : ode_exp(lkf);
     }
+    o.kf = kf;
+    o.Rf = kf * ((C[r0] * C[r1]) * C[r2]);
     const int type = fl & kFlagTypeMask;
     if (type != 0) {
         double thd;
@@ -700,7 +731,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
     double Yk[NS], cpR[NS], hRT[NS], dcpR[NS];
 #pragma unroll 2
     for (int e = lane; e < N * LDA; e += G) A[e] = LinT(0);
-    const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR);
+    const CellThermo c = species_phase<MT>(M, P, y, sm, lane, Yk, cpR, hRT, dcpR, js->H);
     constexpr bool conv = MT::CONV;   // constant volume (see species_phase)
     constexpr int ns = MT::NSLOT;
     const RxnCtx rc = rxn_ctx(c);
@@ -726,7 +757,7 @@ __device__ __noinline__ void warp_jac(double P, const Vec<MT::NS> yv, unsigned A
 #pragma unroll
                 for (int e = 0; e < kJRow; ++e) {
                     const int k = __ldg(M.jrow + e * ns + s);
-                    if (k >= 0) dH += __ldg(M.jnu + e * ns + s) * sm->H[k];
+                    if (k >= 0) dH += __ldg(M.jnu + e * ns + s) * js->H[k];
                 }
                 dlnkr = o.dlnkf_dT - (dH - (double)__ldg(M.dnu + s)) * c.invT;
             }

@@ -106,7 +106,8 @@ __device__ __forceinline__ void lu_trailing_forked(unsigned A_off, int k0, int k
 }
 
 // LU factorization in place (both forms below give the same factors).  perm =
-// the composed row permutation ((P b)[i] = b[perm[i]]); dinv[k] = 1 / U_kk.
+// the composed row permutation ((P b)[i] = b[perm[i]]); the diagonal holds
+// 1 / U_kk (no step reads U_kk once its column's multipliers are formed).
 // Returns 0, or k+1 if U_kk == 0 (singular).  All 32 lanes call it.
 //
 // Blocked form, in LAPACK's getrf order: a panel of kPanel columns is factored with
@@ -123,14 +124,14 @@ __device__ __forceinline__ void lu_trailing_forked(unsigned A_off, int k0, int k
 // once per element (with one warp per SM for the largest mechanisms, nothing
 // else hides it).
 template <class MT, class LinT>
-__device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+__device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off, int lane) {
     static_assert(MT::G == 32, "the blocked LU serves one cell per warp");
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS;
     constexpr int kPanel = 4;                               // panel width
     constexpr int kRows = sizeof(LinT) == 4 ? 8 : 4;        // rows per trailing-update batch
+    static_assert(N <= 256, "perm holds bytes");
     LinT* A = smem_at<LinT>(A_off);
-    int* perm = smem_at<int>(perm_off);
-    LinT* dinv = smem_at<LinT>(dinv_off);
+    unsigned char* perm = smem_at<unsigned char>(perm_off);
     int sing = 0;
     int pv[NS];   // lane tracks perm[i] for i = lane + 32 s
 #pragma unroll
@@ -175,7 +176,6 @@ __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off
                 __syncwarp();
             }
             const LinT inv = LinT(1) / A[k * LDA + k];
-            if (lane == 0) dinv[k] = inv;
             // multipliers (column k below the diagonal), then the panel's
             // columns right of k; lane owns rows i = k + 1 + lane + 32 t
             LinT ukj[kPanel - 1];
@@ -197,7 +197,8 @@ __device__ __forceinline__ int warp_lu_blocked(unsigned A_off, unsigned perm_off
                         if (k + 1 + q < kend && ukj[q] != LinT(0)) A[i * LDA + k + 1 + q] = a[q] - lik * ukj[q];
                 }
             }
-            __syncwarp();
+            __syncwarp();   // every lane has read U_kk
+            if (lane == 0) A[k * LDA + k] = inv;
         }
         if (sing || kend >= N) break;
         // ---- 2. block rows right of the panel: U12 = L11^-1 A12 (lane owns
@@ -254,12 +255,12 @@ constexpr int kBatchedUpdateMinN = 32;
 // the small mechanisms are bound by instruction fetch, where the blocked
 // form's larger code costs more than it saves.
 template <class MT, class LinT>
-__device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
+__device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
     const unsigned gm = gmask<G>();
+    static_assert(N <= 256, "perm holds bytes");
     LinT* A = smem_at<LinT>(A_off);
-    int* perm = smem_at<int>(perm_off);
-    LinT* dinv = smem_at<LinT>(dinv_off);
+    unsigned char* perm = smem_at<unsigned char>(perm_off);
     int sing = 0;
     int pv[NS];   // lane tracks perm[i] for i = lane + G s
 #pragma unroll
@@ -306,9 +307,9 @@ __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off
             __syncwarp(gm);
         }
         const LinT inv = LinT(1) / A[k * LDA + k];
-        if (lane == 0) dinv[k] = inv;
         for (int i = k + 1 + lane; i < N; i += G) A[i * LDA + k] *= inv;
-        __syncwarp(gm);
+        __syncwarp(gm);   // every lane has read U_kk
+        if (lane == 0) A[k * LDA + k] = inv;
         // rank-1 update of the trailing block; lane owns columns j = lane + G s > k.
         if constexpr (N >= kBatchedUpdateMinN) {
             // rows in batches of kRows whose multipliers and entries are all
@@ -372,20 +373,22 @@ __device__ __forceinline__ int warp_lu_compact(unsigned A_off, unsigned perm_off
 constexpr int kBlockedLuMinN = 96;
 
 template <class MT, class LinT>
-__device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, unsigned dinv_off, int lane) {
-    if constexpr (MT::N >= kBlockedLuMinN) return warp_lu_blocked<MT, LinT>(A_off, perm_off, dinv_off, lane);
-    else return warp_lu_compact<MT, LinT>(A_off, perm_off, dinv_off, lane);
+__device__ __noinline__ int warp_lu(unsigned A_off, unsigned perm_off, int lane) {
+    if constexpr (MT::N >= kBlockedLuMinN) return warp_lu_blocked<MT, LinT>(A_off, perm_off, lane);
+    else return warp_lu_compact<MT, LinT>(A_off, perm_off, lane);
 }
+
+// Matrices from this size up take the blocked triangular sweeps.
+constexpr int kBlockedSolveMinN = 64;
 
 // Solve (L U) x = P b.  b: lane elements (FP64, element i = lane + G s) in,
 // solution out.  Arithmetic in LinT.
 template <class MT, class LinT>
-__device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_off, unsigned dinv_off,
+__device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_off,
                                                   const Vec<MT::NS> bv, int lane) {
     constexpr int N = MT::N, LDA = MT::LDA, NS = MT::NS, G = MT::G;
     const LinT* A = smem_at<LinT>(A_off);
-    const int* perm = smem_at<int>(perm_off);
-    const LinT* dinv = smem_at<LinT>(dinv_off);
+    const unsigned char* perm = smem_at<unsigned char>(perm_off);
     const double (&b)[NS] = bv.v;
     Vec<NS> out;
     LinT x[NS];
@@ -402,27 +405,97 @@ __device__ __noinline__ Vec<MT::NS> warp_lu_solve(unsigned A_off, unsigned perm_
         }
         x[s] = (i < N) ? (LinT)v : LinT(0);
     }
-    // forward: unit lower (rolled: this runs every Newton iteration and must
-    // stay small in the instruction cache; loading the next column ahead of
-    // the current one measured slower)
+    // Sweeps of the larger matrices (kBlockedSolveMinN unknowns up) go in
+    // blocks of kB rows: every lane takes the block's kB partial values (one
+    // shuffle latency for the block instead of one per row), solves the block's
+    // kB x kB triangle itself, and applies the block's columns to its own rows
+    // in column order -- each element gets the same fused multiply-adds in the
+    // same order as in the one-column-at-a-time sweep below, so both give the
+    // same bits.  The smaller matrices take the one-column sweep: rolled and
+    // short (this runs every Newton iteration and must stay small in the
+    // instruction cache, and its registers cost the small kernels resident warps).
+    if constexpr (N >= kBlockedSolveMinN) {
+        constexpr int kB = 4;
+        // forward: unit lower
 #pragma unroll 1
-    for (int k = 0; k < N - 1; ++k) {
-        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G);
+        for (int k0 = 0; k0 < N - 1; k0 += kB) {
+            LinT y[kB];
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int i = lane + G * s;
-            if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
+            for (int r = 0; r < kB; ++r) {
+                const int k = k0 + r;
+                y[r] = (k < N) ? group_shfl<G>(pick<NS>(x, k / G), k % G) : LinT(0);
+            }
+#pragma unroll
+            for (int r = 1; r < kB; ++r) {
+                if (k0 + r < N) {
+#pragma unroll
+                    for (int q = 0; q < r; ++q) y[r] -= A[(k0 + r) * LDA + k0 + q] * y[q];
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int i = lane + G * s;
+                if (i >= k0 + kB && i < N) {
+#pragma unroll
+                    for (int q = 0; q < kB; ++q) x[s] -= A[i * LDA + k0 + q] * y[q];
+                }
+#pragma unroll
+                for (int r = 1; r < kB; ++r)
+                    if (i == k0 + r && i < N) x[s] = y[r];
+            }
         }
-    }
-    // backward: upper
+        // backward: upper (the diagonal holds 1 / U_kk)
 #pragma unroll 1
-    for (int k = N - 1; k >= 0; --k) {
-        const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * dinv[k];
-        if (lane == (k % G)) place<NS>(x, k / G, xk);
+        for (int k1 = N - 1; k1 >= 0; k1 -= kB) {
+            LinT y[kB];
 #pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const int i = lane + G * s;
-            if (i < k) x[s] -= A[i * LDA + k] * xk;
+            for (int r = 0; r < kB; ++r) {
+                const int k = k1 - r;
+                y[r] = (k >= 0) ? group_shfl<G>(pick<NS>(x, k / G), k % G) : LinT(0);
+            }
+#pragma unroll
+            for (int r = 0; r < kB; ++r) {
+                const int k = k1 - r;
+                if (k >= 0) {
+#pragma unroll
+                    for (int q = 0; q < r; ++q) y[r] -= A[k * LDA + k1 - q] * y[q];
+                    y[r] = y[r] * A[k * LDA + k];
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int i = lane + G * s;
+                if (i <= k1 - kB) {
+#pragma unroll
+                    for (int q = 0; q < kB; ++q) x[s] -= A[i * LDA + k1 - q] * y[q];
+                }
+#pragma unroll
+                for (int r = 0; r < kB; ++r)
+                    if (i == k1 - r) x[s] = y[r];
+            }
+        }
+    } else {
+        // forward: unit lower (rolled: this runs every Newton iteration and must
+        // stay small in the instruction cache)
+#pragma unroll 1
+        for (int k = 0; k < N - 1; ++k) {
+            const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int i = lane + G * s;
+                if (i > k && i < N) x[s] -= A[i * LDA + k] * xk;
+            }
+        }
+        // backward: upper (the diagonal holds 1 / U_kk)
+#pragma unroll 1
+        for (int k = N - 1; k >= 0; --k) {
+            const LinT xk = group_shfl<G>(pick<NS>(x, k / G), k % G) * A[k * LDA + k];
+            if (lane == (k % G)) place<NS>(x, k / G, xk);
+#pragma unroll
+            for (int s = 0; s < NS; ++s) {
+                const int i = lane + G * s;
+                if (i < k) x[s] -= A[i * LDA + k] * xk;
+            }
         }
     }
     // A species no reaction changes has a zero row in J, so its row of M is

@@ -166,7 +166,7 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, cons
                                         void* stream);
 
 /* Size of the static device scratch of b200ode_integrate_device_noalloc. */
-#define B200ODE_NOALLOC_SCRATCH_BYTES (24u << 20)
+#define B200ODE_NOALLOC_SCRATCH_BYTES (32u << 20)
 
 /* b200ode_integrate_device without any device allocation.  No counterpart in
  * the reference.
@@ -180,19 +180,18 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, cons
  * passes every input and output buffer.  This call makes no cudaMalloc, cudaFree
  * or other allocating call: the work-queue head, the call totals and the
  * per-warp Newton scratch live in one static device array of
- * B200ODE_NOALLOC_SCRATCH_BYTES (24 MiB), which every GPU that loads this
+ * B200ODE_NOALLOC_SCRATCH_BYTES (32 MiB), which every GPU that loads this
  * library keeps until the process exits.
  *
  *  - Always runs the persistent kernel (options.persistent and use_graph are
  *    not used), with the launch shape b200ode_integrate_device would use.  A
- *    launch needs 256 bytes + resident cells x per-cell scratch (16.9 KB for
- *    GRI-Mech 3.0 in mixed precision, 28.1 KB in FP64); one that needs more than
+ *    launch needs 256 bytes + resident cells x per-cell scratch (17.4 KB for
+ *    GRI-Mech 3.0 in mixed precision, 28.6 KB in FP64); one that needs more than
  *    the array is refused with B200ODE_ERR_INVALID and the numbers in
- *    b200ode_last_error().  On a 148-SM B200 the default launches of GRI-Mech
- *    3.0 and the H2 mechanisms (either precision) and of n-dodecane in mixed
- *    precision fit; n-dodecane in FP64 (about 89 KB per cell, two cells per SM)
- *    fits only with options.blocks_per_sm = 1, and the 214-species kerosene
- *    mechanism (208 KB per cell) does not fit.  The number of cells is not
+ *    b200ode_last_error().  On a 148-SM B200 the default launch of every
+ *    compiled-in mechanism and precision fits (the largest: the 214-species
+ *    kerosene mechanism, 148 cells x 210 KB = 31.1 MB, and GRI-Mech 3.0 mixed,
+ *    1,776 resident cells x 17.4 KB = 30.8 MB).  The number of cells is not
  *    limited.
  *  - The first call on a device looks up the array's device address there (and,
  *    with lazy module loading, is when the driver loads this library's kernels
@@ -239,7 +238,8 @@ b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n_cells, 
                                             const double* d_Y, double* d_h_mass, void* stream);
 
 /* Autotuner: integrates a sample of the given cells (the first min(n_cells,
- * 8192), or two per SM for the 214-species mechanism; device buffers as
+ * 192 x SMs), about 16 per resident warp, or two per SM for the 214-species
+ * mechanism; device buffers as
  * b200ode_integrate_device, left unmodified) with the persistent kernel and
  * keeps the fastest choice in the handle's options, which later calls on this
  * handle use.  Stage 1 times every launch shape: 4, 2 or 1 warps (cells) per
