@@ -52,22 +52,23 @@ from hpc_ode_b200 import shard, workloads as W  # noqa: E402
 L2_FLUSH_BYTES = 256 << 20
 # DRAM bytes per cell of one k_bdf launch, from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one mixed-precision capture, divided by its cells):
-# the traffic is the compulsory T/P/Y in + T/Y/status out plus the mechanism
-# tables once, so it scales with the cell count (the kerosene capture, one cell
-# per SM, is table-dominated and is not scaled).  Values: (bytes, summary file).
+# the traffic is the compulsory T/P/Y in + T/Y/status out, the mechanism tables
+# once and register-spill write-backs, taken to scale with the cell count (the
+# kerosene capture, one cell per SM, is table-dominated and is not scaled).
+# Values: (bytes, summary file).
 NCU_DRAM_BYTES_PER_CELL = {
-    "gri30": (762.0, "profiles/k_bdf_gri8k_mixed_full.txt"),
-    "h2o2": (114.0, "profiles/k_bdf_h2_32k_mixed_sections.txt"),
-    "nDodecane_Reitz": (2760.0, "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
+    "gri30": (1175.0, "profiles/k_bdf_gri8k_mixed_full.txt"),
+    "h2o2": (106.0, "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    "nDodecane_Reitz": (3934.0, "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
 }
 # Warp instructions per cell-step of the same captures (smsp__inst_executed.sum /
 # (cells x BDF steps per cell)): scaled by the run's own step count, issued
 # instructions against the SMs' peak issue rate.
 NCU_WARP_INSTR_PER_CELL_STEP = {
-    ("gri30", "mixed"): (25.246e9 / (8192 * 132.98), "profiles/k_bdf_gri8k_mixed_full.txt"),
-    ("h2o2", "mixed"): (118.10e9 / (32768 * 558.06), "profiles/k_bdf_h2_32k_mixed_sections.txt"),
-    ("nDodecane_Reitz", "mixed"): (22.379e9 / (1024 * 551.23), "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
-    (W.ESTIMATE, "mixed"): (29.014e9 / (148 * 662.09), "profiles/k_bdf_kero148_mixed_sections.txt"),
+    ("gri30", "mixed"): (25.660e9 / (8192 * 132.98), "profiles/k_bdf_gri8k_mixed_full.txt"),
+    ("h2o2", "mixed"): (114.22e9 / (32768 * 558.06), "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    ("nDodecane_Reitz", "mixed"): (22.700e9 / (1024 * 551.23), "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
+    (W.ESTIMATE, "mixed"): (27.519e9 / (148 * 662.09), "profiles/k_bdf_kero148_mixed_sections.txt"),
 }
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 CPU_SAMPLE = {"gri_1m": 4096, "gri_bimodal": 8192, "gri_32k": 8192, "h2_1024": 1024, "h2li_grid": 4096,
