@@ -401,12 +401,14 @@ __device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, u
     RxnOut o;
     o.q = 0.0; o.kf = 0.0; o.kr = 0.0; o.Rf = 0.0; o.Rr = 0.0; o.phi = 1.0; o.thd = 0.0;
     o.dphi_dthd = 0.0; o.dphi_dT = 0.0; o.dlnkf_dT = 0.0;
-    const int fl = __ldg(M.flags + s);
+    const uint2 fw = __ldg(M.fac + s);   // factor species, flags, dnu in one word
+    const int fl = (fw.y >> 16) & 511;
     if (!(fl & kFlagActive)) return o;
-    constexpr int ns = MT::NSLOT;
-    const int r0 = __ldg(M.rf + s), r1 = __ldg(M.rf + ns + s), r2 = __ldg(M.rf + 2 * ns + s);
-    const double b = __ldg(M.b + s), EaR = __ldg(M.EaR + s);
-    double lkf = __ldg(M.logA + s) + b * c.logT - EaR * c.invT;
+    static_assert(MT::N < 256, "packed reaction words hold species as bytes");
+    const int r0 = fw.x & 255, r1 = (fw.x >> 8) & 255, r2 = (fw.x >> 16) & 255;
+    const double2 bE = __ldg(M.bEa + s), lP = __ldg(M.lAP + s);
+    const double b = bE.x, EaR = bE.y;
+    double lkf = lP.x + b * c.logT - EaR * c.invT;
     if (deriv) o.dlnkf_dT = (b + EaR * c.invT) * c.invT;
     if constexpr (MT::PLOG) {
         if (fl & kFlagPlog) {   // P = m R T
@@ -418,10 +420,10 @@ __device__ __noinline__ RxnOut rxn_slot(int s, const RxnCtx c, unsigned C_off, u
     const bool constk = fl & kFlagConstK;
     double kf;
     if (fl & kFlagRev) {
-        const int p0 = __ldg(M.pf + s), p1 = __ldg(M.pf + ns + s), p2 = __ldg(M.pf + 2 * ns + s);
-        const int dnu = __ldg(M.dnu + s);
+        const int p0 = fw.x >> 24, p1 = fw.y & 255, p2 = (fw.y >> 8) & 255;
+        const int dnu = (int)(fw.y >> 25) - kFacDnuBias;
         const double sg = (G[p0] + G[p1] + G[p2]) - (G[r0] + G[r1] + G[r2]);
-        const double lnKc = sg - dnu * c.logT + __ldg(M.lnPfac + s);
+        const double lnKc = sg - dnu * c.logT + lP.y;
         double kr;
         if constexpr (MT::N >= kPairedExpMinN) {   // kf's and kr's exponentials in one call
             const Exp2 e = ode_exp2(lkf, constk ? -lnKc : lkf - lnKc);

@@ -17,6 +17,16 @@
 #pragma once
 
 #include <stdint.h>
+#if !defined(__CUDACC__) && !defined(__VECTOR_TYPES_H__)
+// host-only builds without the CUDA headers (the CPU packing checks): the two
+// vector types DevMech's pointers name
+struct uint2 {
+    unsigned int x, y;
+};
+struct alignas(16) double2 {
+    double x, y;
+};
+#endif
 
 #include <algorithm>
 #include <map>
@@ -34,6 +44,13 @@ constexpr int kFlagT2 = 1 << 5;      // Troe with T2 term
 constexpr int kFlagConstK0 = 1 << 6; // k0 = A0
 constexpr int kFlagCatalyst = 1 << 7;  // third body is one species s: [M] = m - sum(C) + C_s
 constexpr int kFlagPlog = 1 << 8;    // pressure-dependent Arrhenius (type 0): kf from the PLOG tables
+
+// Packed reaction word (uint2 per slot, read by the RHS's reaction loop in one
+// load): x = rf0 | rf1 << 8 | rf2 << 16 | pf0 << 24, y = pf1 | pf2 << 8 |
+// flags << 16 (9 bits) | (dnu + 64) << 25; factor species are < 256 (the
+// padding factor is N), dnu in [-64, 63].  The RHS reads (b, EaR) and
+// (logA, lnPfac) as two double2 loads.
+constexpr int kFacDnuBias = 64;
 
 // Species with nonzero net stoichiometry per reaction (rows of jrow / jnu).
 constexpr int kJRow = 8;
@@ -80,6 +97,9 @@ struct DevMech {
     const double* troe_iT3;
     const double* troe_iT1;
     const double* troe_T2;
+    const uint2* fac;       // [nslot] packed factor species, flags, dnu (see kFacDnuBias)
+    const double2* bEa;     // [nslot] (b, EaR)
+    const double2* lAP;     // [nslot] (logA, lnPfac)
     const int* flags;
     const int* rf;          // [3][nslot] reactant factor species (nsp = dummy: C = 1, G = 0)
     const int* pf;          // [3][nslot] product factor species
@@ -127,7 +147,7 @@ struct HostMech {
         o_EaR0, o_A0const, o_troe_a, o_troe_iT3, o_troe_iT1, o_troe_T2, o_flags, o_rf, o_pf,
         o_dnu, o_tb_off, o_tb_len, o_tb_sp, o_tb_alpha, o_jrow, o_jnu, o_sp_off, o_sp_slot,
         o_sp_nu, o_cat_sp, o_gword, o_unit_off, o_plog_lev0, o_plog_nlev, o_plog_lnP, o_plog_toff,
-        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert, o_jword, o_jcoef;
+        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert, o_jword, o_jcoef, o_fac, o_bEa, o_lAP;
     int gmax = 0, nunit = 0, jgmax = 0, njent = 0;
     std::vector<int> jword;      // Jacobian gather (see kJacPieces), also kept for host checks
     std::vector<double> jcoef;
@@ -152,6 +172,9 @@ struct HostMech {
         d.troe_iT3 = (const double*)(base + o_troe_iT3);
         d.troe_iT1 = (const double*)(base + o_troe_iT1);
         d.troe_T2 = (const double*)(base + o_troe_T2);
+        d.fac = (const uint2*)(base + o_fac);
+        d.bEa = (const double2*)(base + o_bEa);
+        d.lAP = (const double2*)(base + o_lAP);
         d.flags = (const int*)(base + o_flags);
         d.rf = (const int*)(base + o_rf);
         d.pf = (const int*)(base + o_pf);
@@ -502,6 +525,31 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
     h.o_inert = PUTV(inert);
     h.o_jword = PUTV(h.jword);
     h.o_jcoef = PUTV(h.jcoef);
+    // the RHS's packed per-slot words
+    std::vector<unsigned> fac(2 * ns);
+    std::vector<double> bEa(2 * ns), lAP(2 * ns);
+    for (int s = 0; s < ns; ++s) {
+        for (int a = 0; a < 3; ++a)
+            if (rf[a * ns + s] < 0 || rf[a * ns + s] > 255 || pf[a * ns + s] < 0 || pf[a * ns + s] > 255) {
+                *err = "mechanism too large for the packed reaction words (256 species)";
+                return HostMech();
+            }
+        if (flags[s] < 0 || flags[s] > 511 || dnu[s] < -kFacDnuBias || dnu[s] >= kFacDnuBias) {
+            *err = "reaction flags or dnu out of the packed word's range";
+            return HostMech();
+        }
+        fac[2 * s] = (unsigned)rf[s] | ((unsigned)rf[ns + s] << 8) | ((unsigned)rf[2 * ns + s] << 16) |
+                     ((unsigned)pf[s] << 24);
+        fac[2 * s + 1] = (unsigned)pf[ns + s] | ((unsigned)pf[2 * ns + s] << 8) | ((unsigned)flags[s] << 16) |
+                         ((unsigned)(dnu[s] + kFacDnuBias) << 25);
+        bEa[2 * s] = b[s];
+        bEa[2 * s + 1] = EaR[s];
+        lAP[2 * s] = logA[s];
+        lAP[2 * s + 1] = lnPfac[s];
+    }
+    h.o_fac = PUTV(fac);
+    h.o_bEa = PUTV(bEa);
+    h.o_lAP = PUTV(lAP);
 #undef PUTV
     h.blob.resize((h.blob.size() + 255) & ~size_t(255));
     return h;

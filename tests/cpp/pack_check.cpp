@@ -119,6 +119,14 @@ static int check(const GenTables& g, int nunits_generated, int nplog_generated) 
     };
     const int* rf = at<int>(h, h.o_rf);
     const int* pf = at<int>(h, h.o_pf);
+    const int* dnu = at<int>(h, h.o_dnu);
+    const double* bb = at<double>(h, h.o_b);
+    const double* EaR = at<double>(h, h.o_EaR);
+    const double* logA = at<double>(h, h.o_logA);
+    const double* lnPfac = at<double>(h, h.o_lnPfac);
+    const unsigned* fac = at<unsigned>(h, h.o_fac);
+    const double* bEa = at<double>(h, h.o_bEa);
+    const double* lAP = at<double>(h, h.o_lAP);
     const int* tb_off = at<int>(h, h.o_tb_off);
     const int* tb_len = at<int>(h, h.o_tb_len);
     const int* tb_sp = at<int>(h, h.o_tb_sp);
@@ -145,6 +153,19 @@ static int check(const GenTables& g, int nunits_generated, int nplog_generated) 
             for (int l = plev0[s]; l < plev0[s] + pnlev[s]; ++l)
                 if (ptoff[l] < 0 || ptoff[l + 1] < ptoff[l] || ptoff[l + 1] > g.nplog_term) return bad("PLOG terms", s, l);
         }
+        // the RHS's packed words decode (as the kernel decodes them) to the same
+        // factor species, flags, dnu, Arrhenius terms and pressure factor
+        const unsigned fx = fac[2 * s], fy = fac[2 * s + 1];
+        const int dec_rf[3] = {(int)(fx & 255), (int)((fx >> 8) & 255), (int)((fx >> 16) & 255)};
+        const int dec_pf[3] = {(int)(fx >> 24), (int)(fy & 255), (int)((fy >> 8) & 255)};
+        for (int a = 0; a < 3; ++a) {
+            if (dec_rf[a] != rf[a * ns + s]) return bad("packed reactant factor", s, dec_rf[a]);
+            if (dec_pf[a] != pf[a * ns + s]) return bad("packed product factor", s, dec_pf[a]);
+        }
+        if ((int)((fy >> 16) & 511) != flags[s]) return bad("packed flags", s, (int)((fy >> 16) & 511));
+        if ((int)(fy >> 25) - b200::kFacDnuBias != dnu[s]) return bad("packed dnu", s, (int)(fy >> 25));
+        if (bEa[2 * s] != bb[s] || bEa[2 * s + 1] != EaR[s] || lAP[2 * s] != logA[s] || lAP[2 * s + 1] != lnPfac[s])
+            return bad("packed Arrhenius / pressure factor", s, 0);
     }
     for (int e = 0; e < h.gmax; ++e)
         for (int l = 0; l < 32; ++l) {
