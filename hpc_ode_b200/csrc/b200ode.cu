@@ -210,7 +210,9 @@ __device__ __forceinline__ void store_cell(const KParams& p, long long cell, int
 // The step code is inlined once, so both forms execute the same instructions
 // and give the same bits.
 // MINB: minimum resident 128-thread blocks per SM the register allocation must
-// allow (1 -> up to 255 registers, 3 -> at most 168); chosen by the autotuner.
+// allow (1 -> up to 255 registers, 3 -> at most 168, 4 -> at most 128: the last
+// only for the mechanisms below kMinb4MaxN unknowns); the host picks the variant
+// that keeps the most CTAs resident, or the options name it.
 // Helper warp of a CTA that integrates one cell of a widest mechanism: runs the
 // shares warp 0 posts until it posts kCmdExit (or, bounded, stops posting).
 template <class MT, class LinT>
@@ -540,8 +542,41 @@ int bdf_occupancy(const b200ode_handle* h, int wpb) {
     return bps;
 }
 
+// The 128-register variant (4 CTAs per SM) is built only below this many
+// unknowns: the H2 kernels fit it with few spills and gain a fourth CTA (16
+// warps per SM: +9 % mixed, +14 % FP64 on 32,768 cells), while larger cells are
+// held to 3 CTAs or fewer by shared memory, where it would only add spills.
+constexpr int kMinb4MaxN = 32;
+
+// Register variant MINB's resident CTAs for wpb warps per CTA (0 for a variant
+// this mechanism does not build).
+template <class MT, class LinT>
+int bdf_variant_occupancy(const b200ode_handle* h, int wpb, int minb) {
+    if (minb == 4) {
+        if constexpr (MT::N < kMinb4MaxN) return bdf_occupancy<MT, LinT, 4>(h, wpb);
+        return 0;
+    }
+    return minb == 3 ? bdf_occupancy<MT, LinT, 3>(h, wpb) : bdf_occupancy<MT, LinT, 1>(h, wpb);
+}
+
+// The register variant (1, 3 or 4) that keeps the most CTAs of wpb warps
+// resident; ties keep the one with more registers a thread.
+template <class MT, class LinT>
+int best_variant(const b200ode_handle* h, int wpb, int* ctas) {
+    int best = 1, occ = bdf_variant_occupancy<MT, LinT>(h, wpb, 1);
+    for (int v : {3, 4}) {
+        const int o = bdf_variant_occupancy<MT, LinT>(h, wpb, v);
+        if (o > occ) {
+            occ = o;
+            best = v;
+        }
+    }
+    if (ctas) *ctas = occ;
+    return best;
+}
+
 // Warps per CTA: the option when set, else the shape (4, 2 or 1 warps per CTA,
-// either register variant) that keeps the most warps resident per SM for this
+// any register variant) that keeps the most warps resident per SM for this
 // mechanism and precision (shared memory per warp and registers decide), ties
 // to the larger CTA.  Computed once per handle.
 template <class MT, class LinT>
@@ -550,7 +585,8 @@ int pick_wpb(b200ode_handle* h) {
     if (h->auto_wpb > 0) return h->auto_wpb;
     int best = 4, best_warps = -1;
     for (int wpb : {4, 2, 1}) {
-        const int bps = std::max(bdf_occupancy<MT, LinT, 1>(h, wpb), bdf_occupancy<MT, LinT, 3>(h, wpb));
+        int bps = 0;
+        best_variant<MT, LinT>(h, wpb, &bps);
         if (bps * wpb > best_warps) {
             best_warps = bps * wpb;
             best = wpb;
@@ -560,22 +596,27 @@ int pick_wpb(b200ode_handle* h) {
     return best;
 }
 
-// The BDF kernel's register variant for wpb warps per CTA: launch bounds of 3
-// CTAs per SM (at most 168 registers a thread) when options.blocks_per_sm asks
-// for that many CTAs, or, with blocks_per_sm = 0, when that variant keeps more
-// CTAs resident than the unconstrained one (decided once per handle and CTA
-// shape; ties keep the unconstrained variant).
+// The BDF kernel's register variant for wpb warps per CTA: with
+// options.blocks_per_sm set, the variant whose launch bounds allow that many
+// CTAs (4 x 4 / wpb or more: 128 registers where built; 3 x 4 / wpb or more:
+// 168), else the one that keeps the most CTAs resident (decided once per
+// handle and CTA shape).
 template <class MT, class LinT>
 auto bdf_kernel(b200ode_handle* h, int wpb) -> void (*)(KParams) {
-    if (h->opt.blocks_per_sm > 0)
-        return h->opt.blocks_per_sm >= 3 * (4 / wpb) ? k_bdf<MT, LinT, 3> : k_bdf<MT, LinT, 1>;
-    const int key = wpb * 1024 + bdf_threads<MT>(h, wpb);
-    auto it = h->auto_minb.find(key);
-    if (it == h->auto_minb.end()) {
-        const bool v3 = bdf_occupancy<MT, LinT, 3>(h, wpb) > bdf_occupancy<MT, LinT, 1>(h, wpb);
-        it = h->auto_minb.emplace(key, v3 ? 3 : 1).first;
+    int v;
+    if (h->opt.blocks_per_sm > 0) {
+        v = h->opt.blocks_per_sm >= 3 * (4 / wpb) ? 3 : 1;
+        if (MT::N < kMinb4MaxN && h->opt.blocks_per_sm >= 4 * (4 / wpb)) v = 4;
+    } else {
+        const int key = wpb * 1024 + bdf_threads<MT>(h, wpb);
+        auto it = h->auto_minb.find(key);
+        if (it == h->auto_minb.end()) it = h->auto_minb.emplace(key, best_variant<MT, LinT>(h, wpb, nullptr)).first;
+        v = it->second;
     }
-    return it->second == 3 ? k_bdf<MT, LinT, 3> : k_bdf<MT, LinT, 1>;
+    if constexpr (MT::N < kMinb4MaxN) {
+        if (v == 4) return k_bdf<MT, LinT, 4>;
+    }
+    return v == 3 ? k_bdf<MT, LinT, 3> : k_bdf<MT, LinT, 1>;
 }
 
 template <class MT, class LinT>
@@ -1302,8 +1343,9 @@ b200ode_status b200ode_autotune(b200ode_handle* h, int64_t n, const double* dP, 
         return B200ODE_OK;
     };
     // stage 1, the launch shape: warps per CTA (4, 2, 1) x register variant
-    // (blocks_per_sm >= 3 * 4 / wpb selects the 168-register variant, which
-    // trades spills for resident warps) x threads per cell for the widest
+    // (blocks_per_sm = 0: the variant that keeps the most CTAs resident;
+    // blocks_per_sm = 3 * 4 / wpb: the 168-register one, which trades spills
+    // for resident warps) x threads per cell for the widest
     // mechanism (a 4-warp CTA per cell with helper warps, or one warp); shapes
     // whose shared memory exceeds a CTA's are skipped
     struct Cand { int wpb, bps, helpers, chunk; };

@@ -76,7 +76,11 @@ typedef struct {
     int32_t refine;           /* mixed only: 1 = one FP64-residual refinement sweep per solve */
     int32_t persistent;       /* 1 = persistent kernel + device work queue; 0 = one launch per BDF step */
     int32_t warps_per_block;  /* 0 = from the autotuner / occupancy */
-    int32_t blocks_per_sm;    /* 0 = from occupancy */
+    int32_t blocks_per_sm;    /* 0 = from occupancy, with the kernel's register variant (up to 255,
+                                 168 or 128 registers a thread; 128 only below 32 unknowns) that
+                                 keeps the most CTAs resident; n >= 3 x 4 / warps_per_block
+                                 selects the 168-register variant, n >= 4 x 4 / warps_per_block
+                                 the 128-register one where built */
     int32_t queue_chunk;      /* persistent form: consecutive cells a warp claims per work-queue
                                  access, 1..64 (0 = 1); larger chunks trade queue traffic for
                                  tail balance.  Results do not depend on it. */
@@ -243,7 +247,8 @@ b200ode_status b200ode_eval_enthalpy_device(b200ode_handle* h, int64_t n_cells, 
  * b200ode_integrate_device, left unmodified) with the persistent kernel and
  * keeps the fastest choice in the handle's options, which later calls on this
  * handle use.  Stage 1 times every launch shape: 4, 2 or 1 warps (cells) per
- * CTA x the full-register or the 168-register kernel variant, and for the
+ * CTA x the register variant that keeps the most CTAs resident or the
+ * 168-register one, and for the
  * 214-species mechanism also the threads per cell (one 4-warp CTA per cell
  * with helper warps, or one warp), skipping shapes whose shared memory exceeds
  * a CTA's; stage 2 times the work-queue chunk (1, 2 or 8 cells per claim) on
