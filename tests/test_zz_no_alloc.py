@@ -86,7 +86,7 @@ def test_noalloc_rejects_bad_arguments():
     (W.ESTIMATE, "kero_2k", native.B200ODE_MIXED, 148),
 ])
 def test_noalloc_takes_every_default_full_launch(mech, wl, precision, ncells):
-    """With enough cells for every resident warp of every SM (at most 12 per SM;
+    """With enough cells for every resident warp of every SM (at most 16 per SM;
     one CTA per cell for the kerosene mechanism) the default launch of each
     compiled-in mechanism needs its largest scratch, and it fits the static
     array: the call is not refused and integrates every cell (a short interval:
