@@ -57,16 +57,16 @@ L2_FLUSH_BYTES = 256 << 20
 # kerosene capture, one cell per SM, is table-dominated and is not scaled).
 # Values: (bytes, summary file).
 NCU_DRAM_BYTES_PER_CELL = {
-    "gri30": (1175.0, "profiles/k_bdf_gri8k_mixed_full.txt"),
-    "h2o2": (106.0, "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    "gri30": (1157.0, "profiles/k_bdf_gri8k_mixed_full.txt"),
+    "h2o2": (148.0, "profiles/k_bdf_h2_32k_mixed_sections.txt"),
     "nDodecane_Reitz": (3934.0, "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
 }
 # Warp instructions per cell-step of the same captures (smsp__inst_executed.sum /
 # (cells x BDF steps per cell)): scaled by the run's own step count, issued
 # instructions against the SMs' peak issue rate.
 NCU_WARP_INSTR_PER_CELL_STEP = {
-    ("gri30", "mixed"): (25.660e9 / (8192 * 132.98), "profiles/k_bdf_gri8k_mixed_full.txt"),
-    ("h2o2", "mixed"): (114.22e9 / (32768 * 558.06), "profiles/k_bdf_h2_32k_mixed_sections.txt"),
+    ("gri30", "mixed"): (25.293e9 / (8192 * 132.98), "profiles/k_bdf_gri8k_mixed_full.txt"),
+    ("h2o2", "mixed"): (122.29e9 / (32768 * 558.06), "profiles/k_bdf_h2_32k_mixed_sections.txt"),
     ("nDodecane_Reitz", "mixed"): (22.700e9 / (1024 * 551.23), "profiles/k_bdf_nc12_1k_mixed_sections.txt"),
     (W.ESTIMATE, "mixed"): (27.519e9 / (148 * 662.09), "profiles/k_bdf_kero148_mixed_sections.txt"),
 }
@@ -268,12 +268,14 @@ def serving_block(native, device: int, n_requests: int, load: float, seed: int =
     reqs = list(W.serving_requests(n_requests, seed=seed, min_cells=min_cells, max_cells=max_cells))
     srv = native.Server(max_inflight=4, device=device, chunk_cells=chunk_cells)
     try:
-        # saturation: the calibration requests submitted at once (also warms handles and staging)
-        t0 = time.perf_counter()
-        ids = [srv.submit(b.mech, b.T.copy(), np.ascontiguousarray(b.Y.copy()), b.P, b.dt) for b in cal]
-        for r in ids:
-            srv.poll(r, -1)
-        sat = len(cal) / (time.perf_counter() - t0)
+        # saturation: the calibration requests submitted at once, twice; the first
+        # pass warms the server's handles and staging, the second is timed
+        for _ in range(2):
+            t0 = time.perf_counter()
+            ids = [srv.submit(b.mech, b.T.copy(), np.ascontiguousarray(b.Y.copy()), b.P, b.dt) for b in cal]
+            for r in ids:
+                srv.poll(r, -1)
+            sat = len(cal) / (time.perf_counter() - t0)
         rate = load * sat
         rng = np.random.default_rng(seed + 7)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
