@@ -156,11 +156,14 @@ struct JacScratch {
 };
 
 // NASA-7 polynomials of species k at T: cp/R, h/RT, s/R - h/RT, d(cp/R)/dT.
+// Coefficients from the species-innermost copy (nasa_sk), so the lanes of a
+// warp, which hold consecutive species, read consecutive words.
 __device__ __forceinline__ void nasa7(const DevMech& M, int k, double T, double logT, double invT,
                                       double& cpR, double& hRT, double& mgRT, double& dcpR) {
-    const double* a = M.nasa + 14 * k + ((T <= __ldg(M.tmid + k)) ? 0 : 7);
-    const double a0 = __ldg(a + 0), a1 = __ldg(a + 1), a2 = __ldg(a + 2), a3 = __ldg(a + 3),
-                 a4 = __ldg(a + 4), a5 = __ldg(a + 5), a6 = __ldg(a + 6);
+    const int nsp = M.nsp;
+    const double* a = M.nasa_sk + ((T <= __ldg(M.tmid + k)) ? 0 : 7) * nsp + k;
+    const double a0 = __ldg(a), a1 = __ldg(a + nsp), a2 = __ldg(a + 2 * nsp), a3 = __ldg(a + 3 * nsp),
+                 a4 = __ldg(a + 4 * nsp), a5 = __ldg(a + 5 * nsp), a6 = __ldg(a + 6 * nsp);
     cpR = a0 + T * (a1 + T * (a2 + T * (a3 + a4 * T)));
     hRT = a0 + T * (a1 * 0.5 + T * (a2 * (1.0 / 3.0) + T * (a3 * 0.25 + a4 * 0.2 * T))) + a5 * invT;
     mgRT = a0 * (logT - 1.0) + T * (a1 * 0.5 + T * (a2 * (1.0 / 6.0) + T * (a3 * (1.0 / 12.0) + a4 * 0.05 * T)))

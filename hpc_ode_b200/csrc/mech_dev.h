@@ -83,6 +83,7 @@ struct DevMech {
     const double* inv_mw;   // [nsp]
     const double* tmid;     // [nsp]
     const double* nasa;     // [nsp][14]: low range a0..a6, high range a0..a6
+    const double* nasa_sk;  // [14][nsp]: the same, species innermost (lane-coalesced)
     // reaction slots [nslot]
     const double* logA;
     const double* b;
@@ -147,7 +148,8 @@ struct HostMech {
         o_EaR0, o_A0const, o_troe_a, o_troe_iT3, o_troe_iT1, o_troe_T2, o_flags, o_rf, o_pf,
         o_dnu, o_tb_off, o_tb_len, o_tb_sp, o_tb_alpha, o_jrow, o_jnu, o_sp_off, o_sp_slot,
         o_sp_nu, o_cat_sp, o_gword, o_unit_off, o_plog_lev0, o_plog_nlev, o_plog_lnP, o_plog_toff,
-        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert, o_jword, o_jcoef, o_fac, o_bEa, o_lAP;
+        o_plog_A, o_plog_logA, o_plog_b, o_plog_EaR, o_inert, o_jword, o_jcoef, o_fac, o_bEa, o_lAP,
+        o_nasa_sk;
     int gmax = 0, nunit = 0, jgmax = 0, njent = 0;
     std::vector<int> jword;      // Jacobian gather (see kJacPieces), also kept for host checks
     std::vector<double> jcoef;
@@ -159,6 +161,7 @@ struct HostMech {
         d.inv_mw = (const double*)(base + o_inv_mw);
         d.tmid = (const double*)(base + o_tmid);
         d.nasa = (const double*)(base + o_nasa);
+        d.nasa_sk = (const double*)(base + o_nasa_sk);
         d.logA = (const double*)(base + o_logA);
         d.b = (const double*)(base + o_b);
         d.EaR = (const double*)(base + o_EaR);
@@ -547,6 +550,10 @@ inline HostMech pack_mechanism(const GenTables& g, std::string* err) {
         lAP[2 * s] = logA[s];
         lAP[2 * s + 1] = lnPfac[s];
     }
+    std::vector<double> nasa_sk(14 * n);
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < 14; ++i) nasa_sk[(size_t)i * n + k] = nasa[14 * k + i];
+    h.o_nasa_sk = PUTV(nasa_sk);
     h.o_fac = PUTV(fac);
     h.o_bEa = PUTV(bEa);
     h.o_lAP = PUTV(lAP);

@@ -125,6 +125,12 @@ static int check(const GenTables& g, int nunits_generated, int nplog_generated) 
     const double* logA = at<double>(h, h.o_logA);
     const double* lnPfac = at<double>(h, h.o_lnPfac);
     const unsigned* fac = at<unsigned>(h, h.o_fac);
+    // the species-innermost NASA-7 copy holds the same coefficients
+    const double* nasa = at<double>(h, h.o_nasa);
+    const double* nasa_sk = at<double>(h, h.o_nasa_sk);
+    for (int k = 0; k < n; ++k)
+        for (int i = 0; i < 14; ++i)
+            if (nasa_sk[(size_t)i * n + k] != nasa[14 * k + i]) return bad("NASA-7 species-innermost copy", k, i);
     const double* bEa = at<double>(h, h.o_bEa);
     const double* lAP = at<double>(h, h.o_lAP);
     const int* tb_off = at<int>(h, h.o_tb_off);
