@@ -1,7 +1,8 @@
 """Generate the golden fixtures under tests/golden/ from the reference.
 
-Run in a checkout that has the reference tree (REF_DIR; default HPC_ODE_REFERENCE,
-else BASELINE.json's reference_path) and its pyJac C built by ``make -C oracle ref``:
+Run in a checkout that has the reference tree (REF_DIR; default oracle/refpath.py's
+reference_dir(): HPC_ODE_REFERENCE, else the checkout's default location) and its pyJac C
+built by ``make -C oracle ref``:
 
     python tests/golden/make_golden.py [REF_DIR]
 
