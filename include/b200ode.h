@@ -197,9 +197,10 @@ b200ode_status b200ode_integrate_device(b200ode_handle* h, int64_t n_cells, cons
  *    kerosene mechanism, 148 cells x 210 KB = 31.1 MB, and GRI-Mech 3.0 mixed,
  *    1,776 resident cells x 17.4 KB = 30.8 MB).  The number of cells is not
  *    limited.
- *  - The first call on a device looks up the array's device address there (and,
- *    with lazy module loading, is when the driver loads this library's kernels
- *    onto that device).  Make that first call before any stream capture.
+ *  - The first call on a device looks up the array's device address there
+ *    (and, with lazy module loading, is when the CUDA driver loads this
+ *    library's kernels onto that device).  Make that first call before any
+ *    stream capture.
  *  - Every call on a device shares the one array, which keeps the previous
  *    call's contents; each call clears the part that must start at zero.  Calls
  *    that overlap on the GPU (different streams, handles or host threads without

@@ -1,7 +1,7 @@
 /* CPU oracle: CVODE-semantics variable-order BDF -- TEST INFRASTRUCTURE ONLY.
  *
- * Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs as
- * the checker; never linked by the product.
+ * Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs to
+ * check results; never linked by the product.
  *
  * Stands in for the reference's serial CVODE integrator
  * (src/Integrators/CVodeIntegrator.cpp:98-155: CVodeCreate(CV_BDF),

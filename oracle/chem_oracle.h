@@ -1,7 +1,7 @@
 /* CPU oracle for the chemistry source terms -- TEST INFRASTRUCTURE ONLY.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs use
- * this code, as the checker.  The product path (hpc_ode_b200/csrc) never
+ * this code, to check results.  The product path (hpc_ode_b200/csrc) never
  * links it.
  *
  * It restates, table-driven, what the reference's pyJac C kernels compute:

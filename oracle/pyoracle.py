@@ -1,7 +1,7 @@
 """ctypes bindings for the CPU oracle -- TEST INFRASTRUCTURE ONLY.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-legs import this module, as the checker.  It loads ``oracle/liboracle.so``
+legs import this module, to check results.  It loads ``oracle/liboracle.so``
 (restated chemistry + CVODE-semantics BDF, built by ``oracle/Makefile``) and,
 when present, ``oracle/_ref/libpyjac_gri30.so`` (the reference's own pyJac C
 kernels compiled from their sources; ``src/Mechanism/CPU``).

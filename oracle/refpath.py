@@ -1,7 +1,7 @@
 """Where the reference checkout lies -- TEST INFRASTRUCTURE ONLY.
 
-The reference (alvarospace/hpc_ode) is read only to build the checker (its
-pyJac C chemistry, oracle/Makefile ``ref``) and to generate golden fixtures; the
+The reference (alvarospace/hpc_ode) is read only to build the oracle's
+reference kernels (its pyJac C chemistry, oracle/Makefile ``ref``) and to generate golden fixtures; the
 GPU path never reads it.  Its location comes from the environment variable
 HPC_ODE_REFERENCE, else the checkout's default location (DEFAULT_REFERENCE);
 None when neither is an existing directory.

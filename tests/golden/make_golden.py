@@ -19,7 +19,7 @@ Writes:
                          of tests/Integrators/data/res_gri_100.csv (gri30).
 
 ``python tests/golden/make_golden.py REF_DIR --only enthalpy`` writes only the last.
-The fixtures are small and committed; the GPU box never reads the reference.
+The fixtures are small and committed; the GPU tests never read the reference.
 """
 from __future__ import annotations
 
