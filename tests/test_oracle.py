@@ -293,3 +293,17 @@ def test_crosscheck_fixture_reproduces(oracle, crosscheck):
             assert np.allclose(r.integrate(dt), crosscheck[f"{wl}_vode"][c], rtol=1e-12, atol=1e-18)
             rr = solve_ivp(f, (0.0, dt), y0[c], method="Radau", jac=J, rtol=1e-10, atol=1e-14)
             assert np.allclose(rr.y[:, -1], crosscheck[f"{wl}_radau"][c], rtol=1e-12, atol=1e-18)
+
+
+def test_reference_location_from_environment(tmp_path, monkeypatch):
+    """The reference checkout the fixture scripts and the oracle's reference build read is
+    HPC_ODE_REFERENCE when set (and an existing directory), and nothing when that names no
+    directory."""
+    from oracle import refpath
+    (tmp_path / "src" / "Mechanism" / "CPU").mkdir(parents=True)
+    monkeypatch.setenv("HPC_ODE_REFERENCE", str(tmp_path))
+    assert refpath.reference_dir() == str(tmp_path)
+    assert refpath.reference_subdir("src", "Mechanism", "CPU") == str(tmp_path / "src" / "Mechanism" / "CPU")
+    assert refpath.reference_subdir("no", "such") is None
+    monkeypatch.setenv("HPC_ODE_REFERENCE", str(tmp_path / "missing"))
+    assert refpath.reference_dir() is None
